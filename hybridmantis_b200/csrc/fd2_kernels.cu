@@ -1,0 +1,614 @@
+// fd2_kernels.cu -- event preparation, photon-count sampling, work-queue
+// construction, the persistent transport kernel and the PHS/Swank pass.
+//
+// Pipeline of one run (all on the context's stream, graph-capturable):
+//   prep      events -> float4 (x, y, z um; history index) + energy     (at submit)
+//   count     N ~ Poisson(E * yield) | Gaussian | given; chunks per event
+//   scan      exclusive scan of chunks per event
+//   fill      chunk descriptors (event, first photon)
+//   transport persistent kernel: warps pull chunks, lanes regenerate photons
+//   phs       per-primary counts -> PHS histogram + FP64 moments (Swank)
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fd2_device.cuh"
+#include "fd2_internal.h"
+
+namespace fd2 {
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ------------------------------------------------------------------ prep
+
+__device__ __forceinline__ bool finite_f(double v) { return isfinite(v); }
+
+__global__ void prep_cm_kernel(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const double *__restrict__ de,
+                               const int32_t *__restrict__ hist, int32_t n_prim, float4 *__restrict__ ev_pos,
+                               double *__restrict__ ev_e, double *__restrict__ ev_xyz, int *status)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        // cm -> um exactly as the reference's host driver (double * 10000.0f),
+        // then the float the transport carries
+        const double xu = x[i] * (double)10000.0f, yu = y[i] * (double)10000.0f, zu = z[i] * (double)10000.0f;
+        const int32_t h = hist[i];
+        const double e = de[i];
+        if (!(finite_f(xu) && finite_f(yu) && finite_f(zu) && finite_f(e)) || e < 0.0 || h < 1 || h > n_prim)
+            atomicOr(status, kStatusBadEvent);
+        ev_pos[i] = make_float4((float)xu, (float)yu, (float)zu, __int_as_float(h - 1));
+        ev_e[i] = e;
+        ev_xyz[3 * i] = xu;
+        ev_xyz[3 * i + 1] = yu;
+        ev_xyz[3 * i + 2] = zu;
+    }
+}
+
+__global__ void prep_um_kernel(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
+                               const float *__restrict__ z, const float *__restrict__ e,
+                               const int32_t *__restrict__ hist, int32_t n_prim, float4 *__restrict__ ev_pos,
+                               double *__restrict__ ev_e, double *__restrict__ ev_xyz, int *status)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t h = hist[i];
+        const double ee = e ? (double)e[i] : 0.0;
+        if (!(isfinite(x[i]) && isfinite(y[i]) && isfinite(z[i]) && isfinite(ee)) || ee < 0.0 || h < 1 || h > n_prim)
+            atomicOr(status, kStatusBadEvent);
+        ev_pos[i] = make_float4(x[i], y[i], z[i], __int_as_float(h - 1));
+        ev_e[i] = ee;
+        ev_xyz[3 * i] = (double)x[i];
+        ev_xyz[3 * i + 1] = (double)y[i];
+        ev_xyz[3 * i + 2] = (double)z[i];
+    }
+}
+
+// ---------------------------------------------------------------- counts
+
+// Uniform double in (0, 1) from two 32-bit words.
+__device__ __forceinline__ double u01d(uint32_t a, uint32_t b)
+{
+    const uint64_t m = ((uint64_t)a << 21) ^ (uint64_t)(b >> 11);  // 53 bits
+    return ((double)(m & ((1ull << 53) - 1)) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+struct CountRng {
+    uint32_t k0, k1, event, tag, block;
+    uint4 buf;
+    int avail;
+    __device__ double u()
+    {
+        if (avail == 0) {
+            buf = philox4x32_10(make_uint4(block++, kCountStream, event, tag), k0, k1);
+            avail = 2;
+        }
+        const double r = avail == 2 ? u01d(buf.x, buf.y) : u01d(buf.z, buf.w);
+        --avail;
+        return r;
+    }
+};
+
+// Poisson(mu): inversion by multiplication for mu < 10; above, the
+// transformed rejection with squeeze PTRS of W. Hormann, "The transformed
+// rejection method for generating Poisson random variables", Insurance:
+// Mathematics and Economics 12 (1993) 39-45.
+__device__ int64_t poisson(CountRng &rng, double mu)
+{
+    if (!(mu > 0.0)) return 0;
+    if (mu < 10.0) {
+        const double limit = exp(-mu);
+        double prod = rng.u();
+        int64_t k = 0;
+        while (prod > limit && k < 1000) {
+            prod *= rng.u();
+            ++k;
+        }
+        return k;
+    }
+    const double smu = sqrt(mu), logmu = log(mu);
+    const double b = 0.931 + 2.53 * smu;
+    const double a = -0.059 + 0.02483 * b;
+    const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int it = 0; it < 10000; ++it) {
+        const double U = rng.u() - 0.5;
+        const double V = rng.u();
+        const double us = 0.5 - fabs(U);
+        const double k = floor((2.0 * a / us + b) * U + mu + 0.43);
+        if (us >= 0.07 && V <= vr) return (int64_t)k;
+        if (k < 0.0 || (us < 0.013 && V > us)) continue;
+        if (log(V) + log(inv_alpha) - log(a / (us * us) + b) <= -mu + k * logmu - lgamma(k + 1.0))
+            return (int64_t)k;
+    }
+    return (int64_t)floor(mu + 0.5);  // unreachable in practice
+}
+
+__global__ void count_kernel(int64_t n, int mode, double yield, int64_t max_per_event, uint64_t seed,
+                             const uint32_t *__restrict__ run_tag_ptr, int chunk, const double *__restrict__ ev_e,
+                             const int32_t *__restrict__ given_n, const uint16_t *__restrict__ ev_geom,
+                             const float4 *__restrict__ ev_pos, int32_t *__restrict__ ev_n,
+                             uint32_t *__restrict__ ev_nchunks, unsigned long long *photons_per_geom,
+                             unsigned long long *photons_total, int32_t *__restrict__ prim_geom, int32_t n_prim,
+                             int *status)
+{
+    const uint32_t run_tag = *run_tag_ptr;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t k;
+        if (mode == kCountGiven) {
+            k = given_n[i];
+        } else {
+            CountRng rng{(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)i, run_tag, 0u, make_uint4(0, 0, 0, 0), 0};
+            const double mu = ev_e[i] * yield;
+            if (mode == kCountGaussian) {
+                const double u1 = rng.u(), u2 = rng.u();
+                const double zn = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+                k = (int64_t)llrint(mu + sqrt(fmax(mu, 0.0)) * zn);
+            } else {
+                k = poisson(rng, mu);
+            }
+        }
+        if (k < 0) k = 0;
+        if (k > max_per_event) {
+            atomicOr(status, kStatusTooManyPhotons);
+            k = 0;
+        }
+        ev_n[i] = (int32_t)k;
+        ev_nchunks[i] = (uint32_t)((k + chunk - 1) / chunk);
+        const int g = ev_geom ? ev_geom[i] : 0;
+        if (k) {
+            atomicAdd(&photons_per_geom[g], (unsigned long long)k);
+            if (photons_total) atomicAdd(&photons_total[g], (unsigned long long)k);
+        }
+        const int32_t prim = __float_as_int(ev_pos[i].w);
+        if (prim_geom && prim >= 0 && prim < n_prim) prim_geom[prim] = g;
+    }
+}
+
+// ------------------------------------------------------------------ scan
+
+constexpr int kScanBlock = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+template <typename T>
+__device__ unsigned long long block_exclusive_scan(unsigned long long v, unsigned long long *warp_sums,
+                                                   unsigned long long *total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned long long s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, s, o);
+            if (lane >= o) s += y;
+        }
+        warp_sums[lane] = s;
+    }
+    __syncthreads();
+    const unsigned long long before = wid ? warp_sums[wid - 1] : 0;
+    *total = warp_sums[(blockDim.x >> 5) - 1];
+    return before + x - v;
+}
+
+// Pass 1: per-tile exclusive scan into offsets, tile totals into block_sums.
+template <typename In>
+__global__ void scan_tiles(int64_t n, const In *__restrict__ in, unsigned long long *__restrict__ out,
+                           unsigned long long *__restrict__ block_sums)
+{
+    __shared__ unsigned long long warp_sums[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    unsigned long long v[kScanItems], sum = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        v[j] = (base + j < n) ? (unsigned long long)in[base + j] : 0ull;
+        sum += v[j];
+    }
+    unsigned long long total;
+    unsigned long long run = block_exclusive_scan<unsigned long long>(sum, warp_sums, &total);
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        if (base + j < n) out[base + j] = run;
+        run += v[j];
+    }
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+// Pass 2: exclusive scan of the tile totals (one CTA, looping).
+__global__ void scan_sums(int64_t tiles, unsigned long long *block_sums, unsigned long long *total)
+{
+    __shared__ unsigned long long warp_sums[32];
+    unsigned long long carry = 0;
+    for (int64_t b = 0; b < tiles; b += blockDim.x) {
+        const int64_t i = b + threadIdx.x;
+        const unsigned long long v = i < tiles ? block_sums[i] : 0ull;
+        unsigned long long t;
+        const unsigned long long ex = block_exclusive_scan<unsigned long long>(v, warp_sums, &t);
+        if (i < tiles) block_sums[i] = carry + ex;
+        carry += t;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// Pass 3: add tile offsets.
+__global__ void scan_add(int64_t n, unsigned long long *__restrict__ out, const unsigned long long *__restrict__ block_sums)
+{
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    const unsigned long long add = block_sums[blockIdx.x];
+    for (int j = threadIdx.x; j < kScanTile; j += blockDim.x)
+        if (base + j < n) out[base + j] += add;
+}
+
+template <typename In>
+cudaError_t scan_impl(cudaStream_t s, int64_t n, const In *in, unsigned long long *offsets,
+                      unsigned long long *block_sums, unsigned long long *total)
+{
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (n > 0) {
+        scan_tiles<In><<<(unsigned)tiles, kScanBlock, 0, s>>>(n, in, offsets, block_sums);
+    }
+    scan_sums<<<1, kScanBlock, 0, s>>>(tiles, block_sums, total);
+    if (n > 0) scan_add<<<(unsigned)tiles, 256, 0, s>>>(n, offsets, block_sums);
+    return cudaGetLastError();
+}
+
+__global__ void fill_chunks_kernel(int64_t n, int chunk, const int32_t *__restrict__ ev_n,
+                                   const unsigned long long *__restrict__ offsets, uint2 *__restrict__ chunks,
+                                   int64_t capacity, int *status)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = ev_n[i];
+        const unsigned long long off = offsets[i];
+        const int32_t nc = (k + chunk - 1) / chunk;
+        if ((int64_t)(off + nc) > capacity) {
+            atomicOr(status, kStatusChunkOverflow);
+            continue;
+        }
+        for (int32_t c = 0; c < nc; ++c) chunks[off + c] = make_uint2((uint32_t)i, (uint32_t)(c * chunk));
+    }
+}
+
+// ------------------------------------------------------------- transport
+
+struct Slot {
+    float4 pos;      // event x, y, z and history index bits
+    uint32_t event;  // event index
+    uint32_t first;  // first photon of the chunk
+    uint32_t count;  // photons in the chunk
+    uint32_t geom;
+};
+constexpr int kRing = 32;
+
+// Persistent transport.  Each warp keeps a ring of up to 32 chunk slots in
+// shared memory, filled with one coalesced load per lane; each lane owns one
+// photon at a time and takes a new one from the ring as soon as (or, with
+// refill > 1, once enough lanes of the warp are) idle, so lanes never wait
+// for the longest walk in the warp.  Fates, per-primary counts and PRF
+// pixels are aggregated across the warp before touching memory; the PRF
+// core of geometry 0 is tallied in a shared-memory window.
+__global__ void __launch_bounds__(1024) transport_kernel(TransportArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    DevGeom *s_geom = reinterpret_cast<DevGeom *>(smem);
+    Slot *s_ring = reinterpret_cast<Slot *>(s_geom + a.n_geom);
+    unsigned int *s_cnt = reinterpret_cast<unsigned int *>(s_ring + nwarps * kRing);
+    float *s_dist = reinterpret_cast<float *>(s_cnt + a.n_geom * kCounterStride);
+    unsigned int *s_win = reinterpret_cast<unsigned int *>(s_dist + a.n_geom);
+
+    for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x) s_geom[i] = a.geoms[i];
+    for (int i = threadIdx.x; i < a.n_geom * kCounterStride; i += blockDim.x) s_cnt[i] = 0;
+    for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x) s_dist[i] = 0.0f;
+    const int win = a.window;
+    for (int i = threadIdx.x; i < win * win; i += blockDim.x) s_win[i] = 0;
+    __syncthreads();
+
+    Slot *ring = s_ring + wid * kRing;
+    // never read past the chunk buffer, whatever the scan produced
+    const unsigned long long total_chunks = min(*a.n_chunks, (unsigned long long)a.chunk_capacity);
+    const uint32_t run_tag = *a.run_tag;
+    int ring_len = 0, slot = 0, refills = 0;
+    uint32_t used = 0;
+    bool exhausted = false, alive = false;
+    const unsigned refill_min = (unsigned)a.refill;
+
+    Photon ph;
+    PhotonRng rng;
+    int prim = 0, geom = 0;
+
+    for (;;) {
+        // ---- hand out photons to idle lanes
+        unsigned needy = __ballot_sync(kFull, !alive);
+        if (needy && !exhausted && ((unsigned)__popc(needy) >= refill_min || needy == kFull)) {
+            while (needy) {
+                if (slot >= ring_len) {
+                    unsigned long long base = 0;
+                    int stop = 0;
+                    if (lane == 0) {
+                        stop = (a.abort_flag && (refills & 15) == 0 && *a.abort_flag) ? 1 : 0;
+                        if (!stop) base = atomicAdd(a.queue_head, (unsigned long long)kRing);
+                    }
+                    ++refills;
+                    stop = __shfl_sync(kFull, stop, 0);
+                    base = __shfl_sync(kFull, base, 0);
+                    if (stop) {
+                        if (lane == 0) atomicOr(a.status, kStatusAborted);
+                        exhausted = true;
+                        break;
+                    }
+                    const unsigned long long idx = base + lane;
+                    const bool ok = idx < total_chunks;
+                    __syncwarp();  // every lane is done reading the old ring
+                    if (ok) {
+                        const uint2 c = a.chunks[idx];
+                        Slot s;
+                        s.pos = a.ev_pos[c.x];
+                        s.event = c.x;
+                        s.first = c.y;
+                        const int32_t n = a.ev_n[c.x];
+                        s.count = (uint32_t)min(a.chunk, n - (int32_t)c.y);
+                        s.geom = a.ev_geom ? a.ev_geom[c.x] : 0;
+                        ring[lane] = s;
+                    }
+                    ring_len = __popc(__ballot_sync(kFull, ok));
+                    __syncwarp();
+                    slot = 0;
+                    used = 0;
+                    if (ring_len == 0) {
+                        exhausted = true;
+                        break;
+                    }
+                }
+                const uint32_t count = ring[slot].count;
+                if (used >= count) {
+                    ++slot;
+                    used = 0;
+                    continue;
+                }
+                const unsigned take = min((unsigned)(count - used), (unsigned)__popc(needy));
+                const unsigned rank = __popc(needy & lanemask_lt());
+                const bool mine = ((needy >> lane) & 1u) && rank < take;
+                if (mine) {
+                    const Slot &s = ring[slot];
+                    const uint32_t k = s.first + used + rank;
+                    ph.ex = s.pos.x; ph.ey = s.pos.y; ph.ez = s.pos.z;
+                    prim = __float_as_int(s.pos.w);
+                    geom = (int)s.geom;
+                    rng.init(a.seed, k, s.event, run_tag);
+                    start_photon(ph, rng, k == 0);
+                    alive = true;
+                }
+                needy &= ~__ballot_sync(kFull, mine);
+                used += take;
+            }
+        }
+        if (__ballot_sync(kFull, alive) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+
+        // ---- one transport step per live lane
+        int fate = kAlive;
+        if (alive) fate = step(ph, rng, s_geom[geom]);
+
+        // ---- warp-aggregated tallies of the photons that ended
+        const unsigned ended = __ballot_sync(kFull, fate != kAlive);
+        if (ended) {
+            if (fate != kAlive) {
+                const unsigned key = (unsigned)(geom * kCounterStride + fate);
+                const unsigned peers = __match_any_sync(ended, key);
+                if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[key], (unsigned)__popc(peers));
+                atomicAdd(&s_dist[geom], ph.dist);
+                alive = false;
+            }
+            const unsigned det = __ballot_sync(kFull, fate == kDetect);
+            if (fate == kDetect) {
+                const unsigned peers = __match_any_sync(det, prim);
+                if (lane == __ffs(peers) - 1 && prim < a.n_prim) atomicAdd(&a.per_primary[prim], __popc(peers));
+                const DevGeom &g = s_geom[geom];
+                if (ph.ii >= 0 && ph.jj >= 0 && ph.ii < g.xdim && ph.jj < g.ydim) {
+                    atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);
+                    const int wx = ph.ii - a.win_x0, wy = ph.jj - a.win_y0;
+                    if (geom == 0 && win > 0 && (unsigned)wx < (unsigned)win && (unsigned)wy < (unsigned)win) {
+                        atomicAdd(&s_win[wx * win + wy], 1u);
+                    } else {
+                        atomicAdd(&a.prf[g.prf_offset + (long long)ph.ii * g.ydim + ph.jj], 1ull);
+                    }
+                }
+            }
+        }
+    }
+
+    // ---- flush the CTA's private tallies
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.n_geom * kCounterStride; i += blockDim.x)
+        if (s_cnt[i]) atomicAdd(&a.counters[i], (unsigned long long)s_cnt[i]);
+    for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x)
+        if (s_dist[i] != 0.0f) atomicAdd(&a.distance[i], (double)s_dist[i]);
+    if (win > 0) {
+        const DevGeom &g = s_geom[0];
+        for (int i = threadIdx.x; i < win * win; i += blockDim.x) {
+            const unsigned v = s_win[i];
+            if (v) {
+                const int ii = a.win_x0 + i / win, jj = a.win_y0 + i % win;
+                atomicAdd(&a.prf[g.prf_offset + (long long)ii * g.ydim + jj], (unsigned long long)v);
+            }
+        }
+    }
+}
+
+// -------------------------------------------------------------------- PHS
+
+// PHS binning of the reference (hybridMANTIS_cuda_ver1_0.cu:376-399) per
+// geometry, plus FP64 moments over histories with >= 1 detected photon.
+__global__ void phs_kernel(int32_t n_prim, const int32_t *__restrict__ per_primary,
+                           const int32_t *__restrict__ prim_geom, int n_geom, int32_t min_photons,
+                           int32_t max_photons, int32_t num_bins, int32_t width, int32_t shift,
+                           int32_t *__restrict__ phs, double *__restrict__ moments,
+                           unsigned long long *dropped)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n_prim; base += stride) {
+        const int64_t i = base + lane;
+        const int32_t c = i < n_prim ? per_primary[i] : 0;
+        const int g = (i < n_prim && prim_geom) ? prim_geom[i] : 0;
+        const bool has = c > 0 && g >= 0 && g < n_geom;
+        if (has) {
+            int32_t bin;
+            if (c <= min_photons) bin = 0;
+            else if (c >= max_photons) bin = num_bins - 1;
+            else bin = c / width - shift;
+            if (bin >= 0 && bin < num_bins) atomicAdd(&phs[(int64_t)g * num_bins + bin], 1);
+            else atomicAdd(&dropped[g], 1ull);
+        }
+        // FP64 moments, summed over the lanes of the warp with the same geometry
+        const unsigned m = __ballot_sync(kFull, has);
+        if (has) {
+            const unsigned peers = __match_any_sync(m, g);
+            const double v1 = (double)c, v2 = (double)c * (double)c;
+            double a1 = 0.0, a2 = 0.0;
+            for (unsigned q = peers; q; q &= q - 1) {
+                const int src = __ffs(q) - 1;
+                a1 += __shfl_sync(peers, v1, src);
+                a2 += __shfl_sync(peers, v2, src);
+            }
+            if (lane == __ffs(peers) - 1) {
+                atomicAdd(&moments[g * 3 + 0], (double)__popc(peers));
+                atomicAdd(&moments[g * 3 + 1], a1);
+                atomicAdd(&moments[g * 3 + 2], a2);
+            }
+        }
+    }
+}
+
+__global__ void bump_kernel(uint32_t *run_tag) { *run_tag += 1u; }
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+
+cudaError_t launch_bump_run_tag(cudaStream_t s, uint32_t *run_tag)
+{
+    bump_kernel<<<1, 1, 0, s>>>(run_tag);
+    return cudaGetLastError();
+}
+
+cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
+{
+    return cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)transport_smem_bytes(cfg, n_geom));
+}
+
+static unsigned grid_for(int64_t n, int block, int cap = 148 * 32)
+{
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+cudaError_t launch_prep_cm(cudaStream_t s, int64_t n, const double *x_cm, const double *y_cm, const double *z_cm,
+                           const double *de, const int32_t *hist, int32_t n_prim, float4 *ev_pos, double *ev_e,
+                           double *ev_xyz, int *status)
+{
+    if (n <= 0) return cudaSuccess;
+    prep_cm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, x_cm, y_cm, z_cm, de, hist, n_prim, ev_pos, ev_e, ev_xyz,
+                                                    status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prep_um(cudaStream_t s, int64_t n, const float *x, const float *y, const float *z, const float *e,
+                           const int32_t *hist, int32_t n_prim, float4 *ev_pos, double *ev_e, double *ev_xyz,
+                           int *status)
+{
+    if (n <= 0) return cudaSuccess;
+    prep_um_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, x, y, z, e, hist, n_prim, ev_pos, ev_e, ev_xyz, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count(cudaStream_t s, int64_t n, int mode, double yield, int64_t max_per_event, uint64_t seed,
+                         const uint32_t *run_tag, int chunk, const double *ev_e, const int32_t *given_n,
+                         const uint16_t *ev_geom, const float4 *ev_pos, int32_t *ev_n, uint32_t *ev_nchunks,
+                         unsigned long long *photons_per_geom, unsigned long long *photons_total,
+                         int32_t *prim_geom, int32_t n_prim, int *status)
+{
+    if (n <= 0) return cudaSuccess;
+    count_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, mode, yield, max_per_event, seed, run_tag, chunk, ev_e, given_n,
+                                                  ev_geom, ev_pos, ev_n, ev_nchunks, photons_per_geom, photons_total,
+                                                  prim_geom, n_prim, status);
+    return cudaGetLastError();
+}
+
+size_t scan_block_sums_needed(int64_t n) { return (size_t)((n + kScanTile - 1) / kScanTile) + 1; }
+
+cudaError_t launch_scan(cudaStream_t s, int64_t n, const uint32_t *in, unsigned long long *offsets,
+                        unsigned long long *block_sums, unsigned long long *total)
+{
+    return scan_impl<uint32_t>(s, n, in, offsets, block_sums, total);
+}
+
+cudaError_t launch_photon_offsets(cudaStream_t s, int64_t n, const int32_t *ev_n, unsigned long long *first,
+                                  unsigned long long *block_sums, unsigned long long *total)
+{
+    return scan_impl<int32_t>(s, n, ev_n, first, block_sums, total);
+}
+
+cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32_t *ev_n,
+                               const unsigned long long *offsets, uint2 *chunks, int64_t capacity, int *status)
+{
+    if (n <= 0) return cudaSuccess;
+    fill_chunks_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, chunk, ev_n, offsets, chunks, capacity, status);
+    return cudaGetLastError();
+}
+
+size_t transport_smem_bytes(const TransportConfig &cfg, int n_geom)
+{
+    const int nwarps = cfg.block / 32;
+    size_t b = sizeof(DevGeom) * (size_t)n_geom + sizeof(Slot) * (size_t)nwarps * kRing +
+               sizeof(unsigned) * (size_t)n_geom * kCounterStride + sizeof(float) * (size_t)n_geom;
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(unsigned) * (size_t)cfg.window * cfg.window;
+    return b;
+}
+
+cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_count, const TransportArgs &a)
+{
+    const size_t smem = transport_smem_bytes(cfg, a.n_geom);
+    const unsigned grid = (unsigned)(sm_count * cfg.ctas_per_sm);
+    transport_kernel<<<grid, cfg.block, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phs(cudaStream_t s, int32_t n_prim, const int32_t *per_primary, const int32_t *prim_geom,
+                       int n_geom, int32_t min_photons, int32_t max_photons, int32_t num_bins, int32_t *phs,
+                       double *moments, unsigned long long *dropped)
+{
+    if (n_prim <= 0) return cudaSuccess;
+    const int32_t width = num_bins > 0 ? (max_photons - min_photons) / num_bins : 0;
+    if (width <= 0) return cudaErrorInvalidValue;
+    const int32_t shift = min_photons / width;
+    phs_kernel<<<grid_for(n_prim, 256, 1024), 256, 0, s>>>(n_prim, per_primary, prim_geom, n_geom, min_photons,
+                                                           max_photons, num_bins, width, shift, phs, moments,
+                                                           dropped);
+    return cudaGetLastError();
+}
+
+}  // namespace fd2

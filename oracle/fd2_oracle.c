@@ -36,6 +36,14 @@
 
 enum { C_GEN, C_DETECT, C_ABS_TOP, C_ABS_BULK, C_LOST, C_OUTOFCOL, C_THETA1 };
 
+/* Call counts of the transport's building blocks (reset by
+ * fd2o_reset_call_counts); used to express the work per photon. */
+static uint64_t o_calls[FD2O_NCALLS];
+#define O_CALL(k) (o_calls[(k)]++)
+
+void fd2o_reset_call_counts(void) { memset(o_calls, 0, sizeof o_calls); }
+void fd2o_get_call_counts(uint64_t out[FD2O_NCALLS]) { memcpy(out, o_calls, sizeof o_calls); }
+
 typedef struct {
     const fd2o_geom *g;
     int32_t seed[2];
@@ -58,6 +66,7 @@ typedef struct {
  * float constant 1/m1 (ranecu, kernel_cuda_c_ver1_0.cu:3694-3710). */
 static float o_u(o_walk *w)
 {
+    O_CALL(FD2O_CALL_UNIFORM);
     int32_t *s = w->seed;
     int32_t k = s[0] / 53668;
     s[0] = O_A1 * (s[0] - k * 53668) - k * 12211;
@@ -152,6 +161,7 @@ static void o_emit(o_walk *w, int first)
  * and u2 (azimuth) (RoughSurface, kernel_cuda_c_ver1_0.cu:3261-3300). */
 static void o_rough(o_walk *w, float beta)
 {
+    O_CALL(FD2O_CALL_ROUGH);
     float *n = w->normal;
     float u = o_u(w);
     float pz = 2.0f * u - 1.0f;
@@ -176,6 +186,7 @@ static void o_rough(o_walk *w, float beta)
  * (trans_dir_cos, kernel_cuda_c_ver1_0.cu:3169-3205). */
 static void o_redirect(o_walk *w, float ti, float tt, int refract)
 {
+    O_CALL(refract ? FD2O_CALL_REFRACT : FD2O_CALL_REFLECT);
     float *d = w->dcos, *n = w->normal;
     float inv[3] = {-d[0], -d[1], -d[2]};
     float ci = o_dot(inv, n);
@@ -244,6 +255,7 @@ static float o_radius(const o_walk *w)
  * the photon is lost or killed out of column. */
 static float o_to_wall(o_walk *w)
 {
+    O_CALL(FD2O_CALL_TO_WALL);
     const fd2o_geom *g = w->g;
     float *p = w->pos, *d = w->dcos;
     const float start[3] = {p[0], p[1], p[2]};
@@ -290,6 +302,7 @@ static float o_to_wall(o_walk *w)
     float step = 0.5f;
     int moved = 0, halved = 0;
     while ((double)r > (double)g->R - 1e-5 && moved < 10 && halved < 10) {
+        O_CALL(FD2O_CALL_PULLBACK);
         float sx = p[0], sy = p[1];
         p[0] = p[0] + step * (-d[0]);
         p[1] = p[1] + step * (-d[1]);
@@ -359,6 +372,7 @@ static int o_next_column_normal(o_walk *w, const float inv[3], int *tries, int a
     const fd2o_geom *g = w->g;
     float *n = w->normal;
     for (;;) {
+        O_CALL(FD2O_CALL_NEW_NORMAL);
         n[0] = inv[0];
         n[1] = inv[1];
         n[2] = inv[2];
@@ -445,6 +459,7 @@ static int o_sensor_between(o_walk *w)
  * 1 = photon ended. */
 static int o_leave_column(o_walk *w, int crosstalk)
 {
+    O_CALL(crosstalk ? FD2O_CALL_CROSSTALK : FD2O_CALL_HOP);
     const fd2o_geom *g = w->g;
     float *p = w->pos, *d = w->dcos;
     float start[3] = {p[0], p[1], p[2]};
@@ -543,6 +558,7 @@ static int o_leave_column(o_walk *w, int crosstalk)
  * kernel_cuda_c_ver1_0.cu:1818-1819 and repeats). */
 static void o_fresnel(float t1, float t2, float *pr, float *pt)
 {
+    O_CALL(FD2O_CALL_FRESNEL);
     double dm = (double)(t1 - t2), dp = (double)(t1 + t2);
     double s2 = sin((double)(2.0f * t1)) * sin((double)(2.0f * t2));
     *pr = (float)(0.5f * ((pow(tan(dm), 2) / pow(tan(dp), 2)) + (pow(sin(dm), 2) / pow(sin(dp), 2))));
@@ -557,6 +573,7 @@ enum { BA_NEW_SURFACE, BA_RESTORE, BA_INCIDENCE };
  * reference's resampling rules.  Returns 1 when the photon ended. */
 static int o_surface(o_walk *w)
 {
+    O_CALL(FD2O_CALL_SURFACE);
     const fd2o_geom *g = w->g;
     float *p = w->pos, *d = w->dcos, *n = w->normal;
     const float half = g->H / 2.0f;
@@ -628,6 +645,7 @@ static int o_surface(o_walk *w)
             stage = BA_INCIDENCE;
         }
         /* BA_INCIDENCE */
+        O_CALL(FD2O_CALL_INCIDENCE);
         for (int k = 0; k < 3; ++k) inv[k] = -d[k];
         t1 = o_dot(inv, n);
         if (t1 > 1.0f || t1 < 0.0f) {
@@ -721,6 +739,7 @@ static void o_restart(o_walk *w)
  * Returns 1 when the photon terminated in this call. */
 static int o_step(o_walk *w)
 {
+    O_CALL(FD2O_CALL_STEP);
     if (w->absorbed == 0) {
         w->bulk_abs = o_flight(w);
         if (w->bulk_abs == 0) w->detect = o_sensor(w);

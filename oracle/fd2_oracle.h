@@ -88,6 +88,16 @@ int fd2o_run(const fd2o_geom *g, int n_events,
              uint64_t *image, int32_t *per_primary, uint64_t *counters,
              int8_t *fate, int32_t *pix, int32_t *seeds, int32_t *steps);
 
+/* Call counts of the transport's building blocks since the last reset,
+ * FD2O_NCALLS entries indexed by FD2O_CALL_*. */
+enum {
+    FD2O_CALL_STEP, FD2O_CALL_TO_WALL, FD2O_CALL_PULLBACK, FD2O_CALL_SURFACE, FD2O_CALL_INCIDENCE,
+    FD2O_CALL_FRESNEL, FD2O_CALL_REFLECT, FD2O_CALL_REFRACT, FD2O_CALL_CROSSTALK, FD2O_CALL_HOP,
+    FD2O_CALL_NEW_NORMAL, FD2O_CALL_ROUGH, FD2O_CALL_UNIFORM, FD2O_NCALLS
+};
+void fd2o_reset_call_counts(void);
+void fd2o_get_call_counts(uint64_t out[FD2O_NCALLS]);
+
 /* RANECU seeds for one stream (init_PRNG, kernel_cuda_c_ver1_0.cu:3516). */
 void fd2o_init_prng(int64_t history_batch, int32_t histories_per_thread,
                     int32_t seed_input, int32_t seed[2]);

@@ -199,6 +199,20 @@ def ranecu(seed, n: int, ref=False):
     return out, seed
 
 
+CALL_NAMES = ["step", "to_wall", "pullback", "surface", "incidence", "fresnel", "reflect", "refract",
+              "crosstalk", "hop", "new_normal", "rough", "uniform"]
+
+
+def reset_call_counts():
+    _load(ORACLE_SO).fd2o_reset_call_counts()
+
+
+def call_counts() -> dict:
+    out = np.zeros(len(CALL_NAMES), np.uint64)
+    _load(ORACLE_SO).fd2o_get_call_counts(_ptr(out, ctypes.c_uint64))
+    return dict(zip(CALL_NAMES, [int(v) for v in out]))
+
+
 def phs(per_primary, min_photons, max_photons, num_bins):
     pp = np.ascontiguousarray(per_primary, dtype=np.int32)
     h = np.zeros(num_bins, np.int32)
