@@ -76,7 +76,7 @@ struct fd2_ctx {
     int *h_abort = nullptr, *d_abort = nullptr;
 
     cudaEvent_t ev_start = nullptr, ev_t0 = nullptr, ev_t1 = nullptr, ev_end = nullptr;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     bool graph_valid = false;
     bool run_pending = false, ran_once = false;
     fd2::TransportConfig cfg;
@@ -332,49 +332,57 @@ cudaError_t count_pass(fd2_ctx *c, bool for_transport)
                              c->d_prim_geom, c->n_prim, c->d_flags);
 }
 
-// The run pipeline, enqueued on the context's stream (captured into the graph).
-cudaError_t enqueue_pipeline(fd2_ctx *c)
+// The run pipeline in three segments on the context's stream: queue build
+// (count, scan, fill), the persistent transport, and the PHS pass.  Each is
+// captured as its own graph; the timing events sit between them.
+cudaError_t enqueue_segment(fd2_ctx *c, int seg)
 {
     const size_t G = c->geoms.size();
-    cudaError_t e = count_pass(c, true);
-    if (e == cudaSuccess)
-        e = fd2::launch_scan(c->stream, c->n_events, c->d_ev_nchunks, c->d_chunk_off, c->d_block_sums, c->d_scalars + 0);
-    if (e == cudaSuccess)
-        e = fd2::launch_fill_chunks(c->stream, c->n_events, c->cfg.chunk, c->d_ev_n, c->d_chunk_off, c->d_chunks,
-                                    c->chunk_cap, c->d_flags);
-    if (e == cudaSuccess) e = cudaEventRecord(c->ev_t0, c->stream);
-    if (e == cudaSuccess) e = fd2::launch_transport(c->stream, c->cfg, c->sm_count, transport_args(c));
-    if (e == cudaSuccess) e = cudaEventRecord(c->ev_t1, c->stream);
-    if (e == cudaSuccess)
+    cudaError_t e = cudaSuccess;
+    if (seg == 0) {
+        e = count_pass(c, true);
+        if (e == cudaSuccess)
+            e = fd2::launch_scan(c->stream, c->n_events, c->d_ev_nchunks, c->d_chunk_off, c->d_block_sums,
+                                 c->d_scalars + 0);
+        if (e == cudaSuccess)
+            e = fd2::launch_fill_chunks(c->stream, c->n_events, c->cfg.chunk, c->d_ev_n, c->d_chunk_off, c->d_chunks,
+                                        c->chunk_cap, c->d_flags);
+    } else if (seg == 1) {
+        e = fd2::launch_transport(c->stream, c->cfg, c->sm_count, transport_args(c));
+    } else {
         e = cudaMemsetAsync(c->d_phs, 0, sizeof(int32_t) * G * (size_t)std::max(c->params.num_bins, 1), c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_moments, 0, sizeof(double) * G * 3, c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_dropped, 0, sizeof(unsigned long long) * G, c->stream);
-    if (e == cudaSuccess && c->params.num_bins > 0 && c->params.max_photons - c->params.min_photons >= c->params.num_bins)
-        e = fd2::launch_phs(c->stream, c->n_prim, c->d_per_primary, c->has_geom ? c->d_prim_geom : nullptr, (int)G,
-                            c->params.min_photons, c->params.max_photons, c->params.num_bins, c->d_phs, c->d_moments,
-                            c->d_dropped);
-    if (e == cudaSuccess) e = fd2::launch_bump_run_tag(c->stream, reinterpret_cast<uint32_t *>(c->d_flags + 1));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->d_moments, 0, sizeof(double) * G * 3, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->d_dropped, 0, sizeof(unsigned long long) * G, c->stream);
+        if (e == cudaSuccess && c->params.num_bins > 0 &&
+            c->params.max_photons - c->params.min_photons >= c->params.num_bins)
+            e = fd2::launch_phs(c->stream, c->n_prim, c->d_per_primary, c->has_geom ? c->d_prim_geom : nullptr, (int)G,
+                                c->params.min_photons, c->params.max_photons, c->params.num_bins, c->d_phs,
+                                c->d_moments, c->d_dropped);
+        if (e == cudaSuccess) e = fd2::launch_bump_run_tag(c->stream, reinterpret_cast<uint32_t *>(c->d_flags + 1));
+    }
     return e;
 }
 
 fd2_status build_graph(fd2_ctx *c)
 {
-    if (c->graph) {
-        cudaGraphExecDestroy(c->graph);
-        c->graph = nullptr;
+    for (auto &g : c->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
     }
-    cudaGraph_t g = nullptr;
-    FD2_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    const cudaError_t e = enqueue_pipeline(c);
-    const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
-    if (e != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        return cuda_fail(c, e, "capture of the run pipeline");
+    for (int seg = 0; seg < 3; ++seg) {
+        cudaGraph_t g = nullptr;
+        FD2_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = enqueue_segment(c, seg);
+        const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(c, e, "capture of the run pipeline");
+        }
+        FD2_CUDA(c, e2);
+        const cudaError_t e3 = cudaGraphInstantiate(&c->graph[seg], g, 0);
+        cudaGraphDestroy(g);
+        FD2_CUDA(c, e3);
     }
-    FD2_CUDA(c, e2);
-    const cudaError_t e3 = cudaGraphInstantiate(&c->graph, g, 0);
-    cudaGraphDestroy(g);
-    FD2_CUDA(c, e3);
     c->graph_valid = true;
     return FD2_OK;
 }
@@ -594,7 +602,8 @@ void fd2_destroy(fd2_ctx *c)
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (auto g : c->graph)
+        if (g) cudaGraphExecDestroy(g);
     dfree(c->d_geoms);
     dfree(c->d_ev_pos);
     dfree(c->d_ev_e);
@@ -789,14 +798,14 @@ fd2_status fd2_run(fd2_ctx *c)
     fd2_status st = ensure_chunks(c);
     if (st != FD2_OK) return st;
     *c->h_abort = 0;
-    FD2_CUDA(c, cudaEventRecord(c->ev_start, c->stream));
-    if (c->opt.use_graph) {
-        if (!c->graph_valid && (st = build_graph(c)) != FD2_OK) return st;
-        FD2_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
-    } else {
-        FD2_CUDA(c, enqueue_pipeline(c));
+    if (c->opt.use_graph && !c->graph_valid && (st = build_graph(c)) != FD2_OK) return st;
+    cudaEvent_t marks[4] = {c->ev_start, c->ev_t0, c->ev_t1, c->ev_end};
+    for (int seg = 0; seg < 3; ++seg) {
+        FD2_CUDA(c, cudaEventRecord(marks[seg], c->stream));
+        if (c->opt.use_graph) FD2_CUDA(c, cudaGraphLaunch(c->graph[seg], c->stream));
+        else FD2_CUDA(c, enqueue_segment(c, seg));
     }
-    FD2_CUDA(c, cudaEventRecord(c->ev_end, c->stream));
+    FD2_CUDA(c, cudaEventRecord(marks[3], c->stream));
     c->run_pending = true;
     c->counts_ready = true;
     c->ran_once = true;

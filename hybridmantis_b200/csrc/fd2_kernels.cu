@@ -302,7 +302,7 @@ constexpr int kRing = 32;
 // for the longest walk in the warp.  Fates, per-primary counts and PRF
 // pixels are aggregated across the warp before touching memory; the PRF
 // core of geometry 0 is tallied in a shared-memory window.
-__global__ void __launch_bounds__(1024) transport_kernel(TransportArgs a)
+__global__ void __launch_bounds__(512) transport_kernel(TransportArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int nwarps = blockDim.x >> 5;
