@@ -7,4 +7,4 @@ from ._lib import Fd2Error, load  # noqa: F401
 from .fastdetect2 import (COUNT_GAUSSIAN, COUNT_GIVEN, COUNT_POISSON, REPLAY_FP64, REPLAY_REF,  # noqa: F401
                           EventSet, OpticalTransport, default_params, params_to_geometry, prf_dims,
                           read_events_binary, read_events_text, read_input_file, synth_events,
-                          write_events_binary, write_events_text)
+                          write_events_binary, write_events_text, write_output_files)

@@ -63,7 +63,7 @@ class Options(ctypes.Structure):
         ("max_photons_per_event", ctypes.c_int64), ("block_size", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32), ("chunk", ctypes.c_int32), ("refill", ctypes.c_int32),
         ("prf_window", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("wait_timeout_s", ctypes.c_double),
-        ("tune_cache", ctypes.c_char_p),
+        ("tune_cache", ctypes.c_char_p), ("event_base", ctypes.c_int64),
     ]
 
 
@@ -106,7 +106,8 @@ EXPORTED = [
     "fd2_set_geometries", "fd2_submit_events", "fd2_submit_events_um", "fd2_run", "fd2_wait",
     "fd2_reset_tallies", "fd2_get_counters", "fd2_get_prf_dims", "fd2_get_prf",
     "fd2_get_detected_per_primary", "fd2_get_photon_counts", "fd2_get_phs", "fd2_get_phs_stats",
-    "fd2_get_timing", "fd2_get_stream", "fd2_write_outputs", "fd2_replay", "fd2_autotune",
+    "fd2_get_timing", "fd2_get_stream", "fd2_write_outputs", "fd2_write_output_files", "fd2_replay",
+    "fd2_autotune",
     "fd2_synth_events", "fd2_free_events", "fd2_read_events_text", "fd2_write_events_text",
     "fd2_read_events_binary", "fd2_write_events_binary",
     "gpuoptical_", "cpuoptical_", "fd2_compat_status",
@@ -150,6 +151,8 @@ def load():
         "fd2_get_timing": (ctypes.c_int, [vp, P(Timing)]),
         "fd2_get_stream": (vp, [vp]),
         "fd2_write_outputs": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "fd2_write_output_files": (ctypes.c_int, [P(Params), P(Geometry), vp, ctypes.c_int32, ctypes.c_int32, vp,
+                                                  ctypes.c_int32, ctypes.c_double, ctypes.c_char_p, ctypes.c_char_p]),
         "fd2_replay": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, vp, vp, vp, vp]),
         "fd2_autotune": (ctypes.c_int, [vp, ctypes.c_int32]),
         "fd2_synth_events": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, P(Events)]),

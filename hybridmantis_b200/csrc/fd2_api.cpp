@@ -264,6 +264,7 @@ fd2_status check_status(fd2_ctx *c)
     if (st & fd2::kStatusTooManyPhotons) return fail(c, FD2_ERR_TOO_MANY_PHOTONS, "an event exceeds max_photons_per_event");
     if (st & fd2::kStatusChunkOverflow) return fail(c, FD2_ERR_OUT_OF_MEMORY, "work-queue capacity exceeded");
     if (st & fd2::kStatusAborted) return fail(c, FD2_ERR_DEVICE_ABORT, "transport aborted");
+    if (st & fd2::kStatusRngUnderflow) return fail(c, FD2_ERR_DEVICE_ABORT, "uniform ring underflow in the walk");
     return FD2_OK;
 }
 
@@ -303,12 +304,21 @@ fd2::TransportArgs transport_args(fd2_ctx *c)
     a.queue_head = c->d_scalars + 1;
     a.geoms = c->d_geoms;
     a.n_geom = (int)c->geoms.size();
+    a.g0 = c->dgeoms[0];
     a.prf = c->d_prf;
     a.per_primary = c->d_per_primary;
     a.n_prim = c->n_prim;
     a.counters = c->d_counters;
     a.distance = c->d_distance;
     a.seed = c->opt.seed;
+    a.event_base = c->opt.event_base;
+    uint32_t k0 = (uint32_t)c->opt.seed, k1 = (uint32_t)(c->opt.seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        a.round_keys[2 * r] = k0;
+        a.round_keys[2 * r + 1] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
     a.run_tag = reinterpret_cast<const uint32_t *>(c->d_flags + 1);
     a.chunk = c->cfg.chunk;
     a.refill = c->cfg.refill;
@@ -325,8 +335,8 @@ cudaError_t count_pass(fd2_ctx *c, bool for_transport)
     const size_t G = c->geoms.size();
     cudaError_t e = cudaMemsetAsync(c->d_scalars, 0, sizeof(unsigned long long) * (3 + G), c->stream);
     if (e != cudaSuccess) return e;
-    return fd2::launch_count(c->stream, c->n_events, c->opt.count_mode, c->params.yield, c->opt.max_photons_per_event,
-                             c->opt.seed, reinterpret_cast<const uint32_t *>(c->d_flags + 1), c->cfg.chunk,
+    return fd2::launch_count(c->stream, c->n_events, c->opt.event_base, c->opt.count_mode, c->params.yield,
+                             c->opt.max_photons_per_event, c->opt.seed, reinterpret_cast<const uint32_t *>(c->d_flags + 1), c->cfg.chunk,
                              c->d_ev_e, c->d_given_n, c->has_geom ? c->d_ev_geom : nullptr, c->d_ev_pos, c->d_ev_n,
                              c->d_ev_nchunks, c->d_scalars + 3, for_transport ? c->d_gen_total : nullptr,
                              c->d_prim_geom, c->n_prim, c->d_flags);
@@ -536,6 +546,7 @@ void fd2_default_options(fd2_options *o)
     o->use_graph = 1;
     o->wait_timeout_s = 0.0;
     o->tune_cache = nullptr;
+    o->event_base = 0;
 }
 
 const char *fd2_last_error(const fd2_ctx *c) { return c ? c->last_error.c_str() : "no context"; }
@@ -552,6 +563,10 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     if (opt) c->opt = *opt;
     else fd2_default_options(&c->opt);
     if (c->opt.max_photons_per_event <= 0) c->opt.max_photons_per_event = 900000;
+    if (c->opt.event_base < 0) {
+        delete c;
+        return FD2_ERR_INVALID_ARGUMENT;
+    }
     if (c->opt.device < 0 || c->opt.device >= ndev || p->num_hist < 0 || !(p->yield >= 0.0)) {
         delete c;
         return FD2_ERR_INVALID_ARGUMENT;
@@ -992,26 +1007,17 @@ fd2_status fd2_write_outputs(fd2_ctx *c, const char *dir)
     const int32_t nb = c->params.num_bins;
     if (nb <= 0 || c->params.max_photons - c->params.min_photons < nb)
         return fail(c, FD2_ERR_INVALID_ARGUMENT, "PHS bin width (max-min)/bins is zero");
-    std::string base(dir);
-    if (!base.empty() && base.back() != '/') base += '/';
     for (size_t g = 0; g < G; ++g) {
         const DevGeom &d = c->dgeoms[g];
         std::vector<uint64_t> img((size_t)d.xdim * d.ydim);
         std::vector<int32_t> phs((size_t)nb);
         if ((st = fd2_get_prf(c, (int32_t)g, img.data(), (int64_t)img.size())) != FD2_OK) return st;
         if ((st = fd2_get_phs(c, (int32_t)g, phs.data(), nb)) != FD2_OK) return st;
-        std::string prf_name = fd2host::output_name(c->params, "myimage_");
-        std::string det_name = fd2host::output_name(c->params, "detected_");
-        if (G > 1) {
-            const std::string suf = "_geom" + std::to_string(g) + ".dat";
-            prf_name = prf_name.substr(0, prf_name.size() - 4) + suf;
-            det_name = det_name.substr(0, det_name.size() - 4) + suf;
-        }
+        const std::string suffix = G > 1 ? "_geom" + std::to_string(g) : std::string();
         const double nh = G > 1 ? std::max(c->hist_per_geom[g], 1.0) : (double)std::max(c->params.num_hist, 1);
-        if ((st = fd2host::write_new_file(base + prf_name, fd2host::format_prf(img.data(), d.xdim, d.ydim, c->geoms[g], nh))) != FD2_OK)
-            return fail(c, st, "writing " + base + prf_name);
-        if ((st = fd2host::write_new_file(base + det_name, fd2host::format_phs(phs.data(), nb))) != FD2_OK)
-            return fail(c, st, "writing " + base + det_name);
+        st = fd2_write_output_files(&c->params, &c->geoms[g], img.data(), d.xdim, d.ydim, phs.data(), nb, nh, dir,
+                                    suffix.c_str());
+        if (st != FD2_OK) return fail(c, st, std::string("writing the output files in ") + dir);
     }
     return FD2_OK;
 }

@@ -28,12 +28,15 @@ struct TransportArgs {
     unsigned long long *queue_head;
     const DevGeom *geoms;
     int n_geom;
+    DevGeom g0;                  // geometry 0 (read from the kernel parameters)
     unsigned long long *prf;     // all geometries' PRF images
     int32_t *per_primary;
     int32_t n_prim;
     unsigned long long *counters;  // [n_geom][kNumFates + 1]: fates, then detected-in-PRF
     double *distance;              // [n_geom]
     uint64_t seed;
+    int64_t event_base;          // global index of event 0 (RNG counters)
+    uint32_t round_keys[20];     // Philox key schedule of the seed
     const uint32_t *run_tag;     // device counter: runs since submission
     int chunk;
     int refill;
@@ -48,7 +51,8 @@ enum : int {
     kStatusTooManyPhotons = 1,
     kStatusBadEvent = 2,
     kStatusAborted = 4,
-    kStatusChunkOverflow = 8
+    kStatusChunkOverflow = 8,
+    kStatusRngUnderflow = 16  // a walk segment drew more uniforms than buffered
 };
 
 constexpr int kCounterStride = kNumFates + 1;
@@ -63,7 +67,7 @@ cudaError_t launch_prep_cm(cudaStream_t s, int64_t n, const double *x_cm, const 
 cudaError_t launch_prep_um(cudaStream_t s, int64_t n, const float *x, const float *y, const float *z,
                            const float *e, const int32_t *hist, int32_t n_prim, float4 *ev_pos,
                            double *ev_e, double *ev_xyz, int *status);
-cudaError_t launch_count(cudaStream_t s, int64_t n, int mode, double yield, int64_t max_per_event,
+cudaError_t launch_count(cudaStream_t s, int64_t n, int64_t event_base, int mode, double yield, int64_t max_per_event,
                          uint64_t seed, const uint32_t *run_tag, int chunk, const double *ev_e,
                          const int32_t *given_n, const uint16_t *ev_geom, const float4 *ev_pos,
                          int32_t *ev_n, uint32_t *ev_nchunks, unsigned long long *photons_per_geom,

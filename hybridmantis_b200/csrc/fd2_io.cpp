@@ -282,6 +282,27 @@ fd2_status fd2_read_events_binary(const char *path, fd2_events *out)
     return FD2_OK;
 }
 
+fd2_status fd2_write_output_files(const fd2_params *p, const fd2_geometry *g, const uint64_t *image, int32_t xdim,
+                                  int32_t ydim, const int32_t *phs, int32_t num_bins, double num_hist, const char *dir,
+                                  const char *suffix)
+{
+    if (!p || !g || !image || !phs || !dir || xdim <= 0 || ydim <= 0 || num_bins <= 0 || !(num_hist > 0.0))
+        return FD2_ERR_INVALID_ARGUMENT;
+    fd2_params q = *p;
+    fd2_params_fill_tags(&q);
+    std::string base(dir);
+    if (!base.empty() && base.back() != '/') base += '/';
+    std::string prf_name = fd2host::output_name(q, "myimage_");
+    std::string det_name = fd2host::output_name(q, "detected_");
+    if (suffix && *suffix) {
+        prf_name = prf_name.substr(0, prf_name.size() - 4) + suffix + ".dat";
+        det_name = det_name.substr(0, det_name.size() - 4) + suffix + ".dat";
+    }
+    fd2_status st = fd2host::write_new_file(base + prf_name, fd2host::format_prf(image, xdim, ydim, *g, num_hist));
+    if (st != FD2_OK) return st;
+    return fd2host::write_new_file(base + det_name, fd2host::format_phs(phs, num_bins));
+}
+
 }  // extern "C"
 
 namespace fd2host {

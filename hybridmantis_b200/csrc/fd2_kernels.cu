@@ -10,6 +10,7 @@
 //   phs       per-primary counts -> PHS histogram + FP64 moments (Swank)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "fd2_device.cuh"
@@ -131,7 +132,7 @@ __device__ int64_t poisson(CountRng &rng, double mu)
     return (int64_t)floor(mu + 0.5);  // unreachable in practice
 }
 
-__global__ void count_kernel(int64_t n, int mode, double yield, int64_t max_per_event, uint64_t seed,
+__global__ void count_kernel(int64_t n, int64_t event_base, int mode, double yield, int64_t max_per_event, uint64_t seed,
                              const uint32_t *__restrict__ run_tag_ptr, int chunk, const double *__restrict__ ev_e,
                              const int32_t *__restrict__ given_n, const uint16_t *__restrict__ ev_geom,
                              const float4 *__restrict__ ev_pos, int32_t *__restrict__ ev_n,
@@ -145,7 +146,8 @@ __global__ void count_kernel(int64_t n, int mode, double yield, int64_t max_per_
         if (mode == kCountGiven) {
             k = given_n[i];
         } else {
-            CountRng rng{(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)i, run_tag, 0u, make_uint4(0, 0, 0, 0), 0};
+            CountRng rng{(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(event_base + i), run_tag, 0u,
+                         make_uint4(0, 0, 0, 0), 0};
             const double mu = ev_e[i] * yield;
             if (mode == kCountGaussian) {
                 const double u1 = rng.u(), u2 = rng.u();
@@ -295,42 +297,78 @@ struct Slot {
 };
 constexpr int kRing = 32;
 
+// Shared-memory layout of the transport kernel (dynamic).
+struct SmemLayout {
+    size_t geom, ring, cnt, dist, win, uring, total;
+    __host__ __device__ SmemLayout(int block, int n_geom, int window)
+    {
+        size_t o = 0;
+        geom = o;
+        o += sizeof(DevGeom) * (size_t)n_geom;
+        o = (o + 15) & ~(size_t)15;
+        ring = o;
+        o += sizeof(Slot) * (size_t)(block / 32) * kRing;
+        cnt = o;
+        o += sizeof(unsigned) * (size_t)n_geom * kCounterStride;
+        dist = o;
+        o += sizeof(float) * (size_t)n_geom;
+        o = (o + 15) & ~(size_t)15;
+        win = o;
+        o += sizeof(unsigned) * (size_t)window * window;
+        uring = o;
+        o += sizeof(float) * (size_t)kURing * block;
+        total = o;
+    }
+};
+
 // Persistent transport.  Each warp keeps a ring of up to 32 chunk slots in
 // shared memory, filled with one coalesced load per lane; each lane owns one
 // photon at a time and takes a new one from the ring as soon as (or, with
 // refill > 1, once enough lanes of the warp are) idle, so lanes never wait
 // for the longest walk in the warp.  Fates, per-primary counts and PRF
 // pixels are aggregated across the warp before touching memory; the PRF
-// core of geometry 0 is tallied in a shared-memory window.
-__global__ void __launch_bounds__(512) transport_kernel(TransportArgs a)
+// core of geometry 0 is tallied in a shared-memory window.  kMulti: the
+// geometry of each photon comes from the table in shared memory; otherwise
+// the single geometry is read from the kernel parameters.
+template <bool kMulti, int kMaxThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(const __grid_constant__ TransportArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int nwarps = blockDim.x >> 5;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    DevGeom *s_geom = reinterpret_cast<DevGeom *>(smem);
-    Slot *s_ring = reinterpret_cast<Slot *>(s_geom + a.n_geom);
-    unsigned int *s_cnt = reinterpret_cast<unsigned int *>(s_ring + nwarps * kRing);
-    float *s_dist = reinterpret_cast<float *>(s_cnt + a.n_geom * kCounterStride);
-    unsigned int *s_win = reinterpret_cast<unsigned int *>(s_dist + a.n_geom);
+    const int win = a.window;
+    const SmemLayout L(blockDim.x, a.n_geom, win);
+    DevGeom *s_geom = reinterpret_cast<DevGeom *>(smem + L.geom);
+    Slot *s_ring = reinterpret_cast<Slot *>(smem + L.ring);
+    unsigned int *s_cnt = reinterpret_cast<unsigned int *>(smem + L.cnt);
+    float *s_dist = reinterpret_cast<float *>(smem + L.dist);
+    unsigned int *s_win = reinterpret_cast<unsigned int *>(smem + L.win);
+    float *s_uring = reinterpret_cast<float *>(smem + L.uring);
+    (void)nwarps;
 
-    for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x) s_geom[i] = a.geoms[i];
+    if (kMulti)
+        for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x) s_geom[i] = a.geoms[i];
     for (int i = threadIdx.x; i < a.n_geom * kCounterStride; i += blockDim.x) s_cnt[i] = 0;
     for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x) s_dist[i] = 0.0f;
-    const int win = a.window;
     for (int i = threadIdx.x; i < win * win; i += blockDim.x) s_win[i] = 0;
     __syncthreads();
 
     Slot *ring = s_ring + wid * kRing;
     // never read past the chunk buffer, whatever the scan produced
     const unsigned long long total_chunks = min(*a.n_chunks, (unsigned long long)a.chunk_capacity);
-    const uint32_t run_tag = *a.run_tag;
     int ring_len = 0, slot = 0, refills = 0;
     uint32_t used = 0;
     bool exhausted = false, alive = false;
     const unsigned refill_min = (unsigned)a.refill;
 
-    Photon ph;
-    PhotonRng rng;
+    __shared__ RngKey s_key;
+    if (threadIdx.x < 20) s_key.rk[threadIdx.x] = a.round_keys[threadIdx.x];
+    if (threadIdx.x == 0) s_key.run = *a.run_tag;
+    __syncthreads();
+    Walker w;
+    w.ring = s_uring + threadIdx.x;
+    w.stride = blockDim.x;
+    w.key = &s_key;
     int prim = 0, geom = 0;
 
     for (;;) {
@@ -364,7 +402,7 @@ __global__ void __launch_bounds__(512) transport_kernel(TransportArgs a)
                         s.first = c.y;
                         const int32_t n = a.ev_n[c.x];
                         s.count = (uint32_t)min(a.chunk, n - (int32_t)c.y);
-                        s.geom = a.ev_geom ? a.ev_geom[c.x] : 0;
+                        s.geom = (kMulti && a.ev_geom) ? a.ev_geom[c.x] : 0;
                         ring[lane] = s;
                     }
                     ring_len = __popc(__ballot_sync(kFull, ok));
@@ -388,11 +426,10 @@ __global__ void __launch_bounds__(512) transport_kernel(TransportArgs a)
                 if (mine) {
                     const Slot &s = ring[slot];
                     const uint32_t k = s.first + used + rank;
-                    ph.ex = s.pos.x; ph.ey = s.pos.y; ph.ez = s.pos.z;
+                    w.ex = s.pos.x; w.ey = s.pos.y; w.ez = s.pos.z;
                     prim = __float_as_int(s.pos.w);
                     geom = (int)s.geom;
-                    rng.init(a.seed, k, s.event, run_tag);
-                    start_photon(ph, rng, k == 0);
+                    w.start(k, (uint32_t)(a.event_base + s.event), k == 0);
                     alive = true;
                 }
                 needy &= ~__ballot_sync(kFull, mine);
@@ -406,30 +443,33 @@ __global__ void __launch_bounds__(512) transport_kernel(TransportArgs a)
 
         // ---- one transport step per live lane
         int fate = kAlive;
-        if (alive) fate = step(ph, rng, s_geom[geom]);
+        if (alive) fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
 
         // ---- warp-aggregated tallies of the photons that ended
         const unsigned ended = __ballot_sync(kFull, fate != kAlive);
         if (ended) {
             if (fate != kAlive) {
+                if (w.underflow) atomicOr(a.status, kStatusRngUnderflow);
                 const unsigned key = (unsigned)(geom * kCounterStride + fate);
                 const unsigned peers = __match_any_sync(ended, key);
                 if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[key], (unsigned)__popc(peers));
-                atomicAdd(&s_dist[geom], ph.dist);
+                atomicAdd(&s_dist[geom], w.dist);
                 alive = false;
             }
             const unsigned det = __ballot_sync(kFull, fate == kDetect);
             if (fate == kDetect) {
                 const unsigned peers = __match_any_sync(det, prim);
                 if (lane == __ffs(peers) - 1 && prim < a.n_prim) atomicAdd(&a.per_primary[prim], __popc(peers));
-                const DevGeom &g = s_geom[geom];
-                if (ph.ii >= 0 && ph.jj >= 0 && ph.ii < g.xdim && ph.jj < g.ydim) {
+                const int xdim = kMulti ? s_geom[geom].xdim : a.g0.xdim;
+                const int ydim = kMulti ? s_geom[geom].ydim : a.g0.ydim;
+                if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {
                     atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);
-                    const int wx = ph.ii - a.win_x0, wy = ph.jj - a.win_y0;
+                    const int wx = w.ii - a.win_x0, wy = w.jj - a.win_y0;
                     if (geom == 0 && win > 0 && (unsigned)wx < (unsigned)win && (unsigned)wy < (unsigned)win) {
                         atomicAdd(&s_win[wx * win + wy], 1u);
                     } else {
-                        atomicAdd(&a.prf[g.prf_offset + (long long)ph.ii * g.ydim + ph.jj], 1ull);
+                        const long long off = kMulti ? s_geom[geom].prf_offset : a.g0.prf_offset;
+                        atomicAdd(&a.prf[off + (long long)w.ii * ydim + w.jj], 1ull);
                     }
                 }
             }
@@ -443,12 +483,13 @@ __global__ void __launch_bounds__(512) transport_kernel(TransportArgs a)
     for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x)
         if (s_dist[i] != 0.0f) atomicAdd(&a.distance[i], (double)s_dist[i]);
     if (win > 0) {
-        const DevGeom &g = s_geom[0];
+        const long long off = kMulti ? s_geom[0].prf_offset : a.g0.prf_offset;
+        const int ydim = kMulti ? s_geom[0].ydim : a.g0.ydim;
         for (int i = threadIdx.x; i < win * win; i += blockDim.x) {
             const unsigned v = s_win[i];
             if (v) {
                 const int ii = a.win_x0 + i / win, jj = a.win_y0 + i % win;
-                atomicAdd(&a.prf[g.prf_offset + (long long)ii * g.ydim + jj], (unsigned long long)v);
+                atomicAdd(&a.prf[off + (long long)ii * ydim + jj], (unsigned long long)v);
             }
         }
     }
@@ -511,12 +552,6 @@ cudaError_t launch_bump_run_tag(cudaStream_t s, uint32_t *run_tag)
     return cudaGetLastError();
 }
 
-cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
-{
-    return cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)transport_smem_bytes(cfg, n_geom));
-}
-
 static unsigned grid_for(int64_t n, int block, int cap = 148 * 32)
 {
     int64_t g = (n + block - 1) / block;
@@ -544,14 +579,14 @@ cudaError_t launch_prep_um(cudaStream_t s, int64_t n, const float *x, const floa
     return cudaGetLastError();
 }
 
-cudaError_t launch_count(cudaStream_t s, int64_t n, int mode, double yield, int64_t max_per_event, uint64_t seed,
+cudaError_t launch_count(cudaStream_t s, int64_t n, int64_t event_base, int mode, double yield, int64_t max_per_event, uint64_t seed,
                          const uint32_t *run_tag, int chunk, const double *ev_e, const int32_t *given_n,
                          const uint16_t *ev_geom, const float4 *ev_pos, int32_t *ev_n, uint32_t *ev_nchunks,
                          unsigned long long *photons_per_geom, unsigned long long *photons_total,
                          int32_t *prim_geom, int32_t n_prim, int *status)
 {
     if (n <= 0) return cudaSuccess;
-    count_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, mode, yield, max_per_event, seed, run_tag, chunk, ev_e, given_n,
+    count_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, event_base, mode, yield, max_per_event, seed, run_tag, chunk, ev_e, given_n,
                                                   ev_geom, ev_pos, ev_n, ev_nchunks, photons_per_geom, photons_total,
                                                   prim_geom, n_prim, status);
     return cudaGetLastError();
@@ -579,21 +614,46 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
     return cudaGetLastError();
 }
 
+// Register budgets: blocks of up to 256 threads are compiled for 2, 3 or 4
+// resident CTAs per SM (128, 85, 64 registers); larger blocks for one.
+#define FD2_TRANSPORT_VARIANTS(X)        \
+    X(false, 512, 1) X(false, 256, 2)    \
+    X(false, 256, 3) X(false, 256, 4)    \
+    X(true, 512, 1) X(true, 256, 2) X(true, 256, 3)
+
+cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
+{
+    const int bytes = (int)transport_smem_bytes(cfg, n_geom);
+    cudaError_t e = cudaSuccess;
+#define FD2_SET_ATTR(M, T, B)                                                                                   \
+    if (e == cudaSuccess)                                                                                       \
+        e = cudaFuncSetAttribute(transport_kernel<M, T, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    FD2_TRANSPORT_VARIANTS(FD2_SET_ATTR)
+#undef FD2_SET_ATTR
+    return e;
+}
+
 size_t transport_smem_bytes(const TransportConfig &cfg, int n_geom)
 {
-    const int nwarps = cfg.block / 32;
-    size_t b = sizeof(DevGeom) * (size_t)n_geom + sizeof(Slot) * (size_t)nwarps * kRing +
-               sizeof(unsigned) * (size_t)n_geom * kCounterStride + sizeof(float) * (size_t)n_geom;
-    b = (b + 15) & ~(size_t)15;
-    b += sizeof(unsigned) * (size_t)cfg.window * cfg.window;
-    return b;
+    return SmemLayout(cfg.block, n_geom, cfg.window).total;
 }
 
 cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_count, const TransportArgs &a)
 {
     const size_t smem = transport_smem_bytes(cfg, a.n_geom);
     const unsigned grid = (unsigned)(sm_count * cfg.ctas_per_sm);
-    transport_kernel<<<grid, cfg.block, smem, s>>>(a);
+    const bool multi = a.n_geom > 1;
+    const int per_sm = cfg.block > 256 ? 1 : std::min(std::max(cfg.ctas_per_sm, 2), multi ? 3 : 4);
+    if (!multi) {
+        if (per_sm == 1) transport_kernel<false, 512, 1><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 2) transport_kernel<false, 256, 2><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 3) transport_kernel<false, 256, 3><<<grid, cfg.block, smem, s>>>(a);
+        else transport_kernel<false, 256, 4><<<grid, cfg.block, smem, s>>>(a);
+    } else {
+        if (per_sm == 1) transport_kernel<true, 512, 1><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 2) transport_kernel<true, 256, 2><<<grid, cfg.block, smem, s>>>(a);
+        else transport_kernel<true, 256, 3><<<grid, cfg.block, smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 

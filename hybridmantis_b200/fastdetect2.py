@@ -21,7 +21,7 @@ from ._lib import (COUNT_GAUSSIAN, COUNT_GIVEN, COUNT_POISSON, REPLAY_FP64, REPL
 
 __all__ = ["read_input_file", "default_params", "params_to_geometry", "prf_dims", "EventSet", "synth_events",
            "OpticalTransport", "Fd2Error", "COUNT_POISSON", "COUNT_GAUSSIAN", "COUNT_GIVEN",
-           "REPLAY_REF", "REPLAY_FP64", "read_events_text", "write_events_text", "read_events_binary",
+           "REPLAY_REF", "REPLAY_FP64", "write_output_files", "read_events_text", "write_events_text", "read_events_binary",
            "write_events_binary"]
 
 
@@ -120,6 +120,16 @@ def read_events_binary(path: str) -> EventSet:
     return _events_from_struct(ev)
 
 
+def write_output_files(params: Params, geometry: Geometry, image, phs, num_hist: float, directory: str,
+                       suffix: str = "") -> None:
+    """detected_*.dat and myimage_*.dat from host arrays (reference formats)."""
+    img = np.ascontiguousarray(image, dtype=np.uint64)
+    ph = np.ascontiguousarray(phs, dtype=np.int32)
+    check(load().fd2_write_output_files(ctypes.byref(params), ctypes.byref(geometry), ptr(img), img.shape[0],
+                                        img.shape[1], ptr(ph), len(ph), float(num_hist), str(directory).encode(),
+                                        suffix.encode()), "write_output_files")
+
+
 def _as_struct(es: EventSet):
     keep = [np.ascontiguousarray(a) for a in (es.x_um, es.y_um, es.z_um, es.e_ev)]
     h = np.ascontiguousarray(es.hist, dtype=np.int32)
@@ -151,7 +161,7 @@ class OpticalTransport:
     def __init__(self, params: Params, *, device: int = 0, count_mode: int = COUNT_POISSON, seed: int | None = None,
                  block_size: int = 0, ctas_per_sm: int = 0, chunk: int = 0, refill: int = 0, prf_window: int = -1,
                  use_graph: bool = True, wait_timeout_s: float = 0.0, max_photons_per_event: int = 900000,
-                 tune_cache: str | None = None):
+                 tune_cache: str | None = None, event_base: int = 0):
         lib = load()
         self._lib = lib
         opt = Options()
@@ -165,6 +175,7 @@ class OpticalTransport:
         opt.use_graph = 1 if use_graph else 0
         opt.wait_timeout_s = wait_timeout_s
         opt.max_photons_per_event = max_photons_per_event
+        opt.event_base = event_base
         self._tune_cache = tune_cache.encode() if tune_cache else None
         opt.tune_cache = self._tune_cache
         self.params = params

@@ -120,6 +120,9 @@ typedef struct fd2_options {
     int32_t use_graph;             /* replay the pipeline as one CUDA graph      */
     double wait_timeout_s;         /* fd2_wait deadline; <= 0 = none             */
     const char *tune_cache;        /* autotuner cache file (JSON), may be NULL   */
+    int64_t event_base;            /* global index of the first submitted event: a
+                                      shard of a larger stream draws the same
+                                      random numbers as in the unsharded run     */
 } fd2_options;
 
 typedef struct fd2_counters {
@@ -200,6 +203,13 @@ FD2_API void *fd2_get_stream(fd2_ctx *ctx);
 /* detected_<tags>.dat and myimage_<tags>.dat in dir, in the reference's
  * formats; fails with FD2_ERR_FILE_EXISTS if either file exists. */
 FD2_API fd2_status fd2_write_outputs(fd2_ctx *ctx, const char *dir);
+
+/* The same two files from host arrays (e.g. tallies merged across GPUs):
+ * image is xdim*ydim counts [ii*ydim + jj], phs num_bins rows, PRF values
+ * divided by num_hist.  suffix (may be NULL) is inserted before ".dat". */
+FD2_API fd2_status fd2_write_output_files(const fd2_params *p, const fd2_geometry *g, const uint64_t *image,
+                                          int32_t xdim, int32_t ydim, const int32_t *phs, int32_t num_bins,
+                                          double num_hist, const char *dir, const char *suffix);
 
 /* FP64/reference-arithmetic replay of the reference C path: RANECU stream
  * init_PRNG(event_index_base + e, 50000, seed_input) per event, photon counts
