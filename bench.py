@@ -348,7 +348,8 @@ def run_ours(a, rank, world, local_rank):
                        "photons_per_step": photons / max(a.steps, 1) / world,
                        "l2": "256 MiB buffer written between timed steps (inside the timed region)",
                        "parallelism": f"weak-scaling x{world}" if world > 1 else "single GPU",
-                       "launch": {k: tm[k] for k in ("grid", "block", "chunk", "refill", "prf_window")}},
+                       "launch": {k: tm[k] for k in ("grid", "block", "chunk", "refill", "prf_window",
+                                                           "fresnel_batch")}},
             "e2e": {"value": e2e_photons / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": a.steps * 9,

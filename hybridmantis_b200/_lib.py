@@ -63,7 +63,8 @@ class Options(ctypes.Structure):
         ("max_photons_per_event", ctypes.c_int64), ("block_size", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32), ("chunk", ctypes.c_int32), ("refill", ctypes.c_int32),
         ("prf_window", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("wait_timeout_s", ctypes.c_double),
-        ("tune_cache", ctypes.c_char_p), ("event_base", ctypes.c_int64),
+        ("tune_cache", ctypes.c_char_p), ("event_base", ctypes.c_int64), ("fresnel_batch", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -84,7 +85,7 @@ class PhsStats(ctypes.Structure):
 class Timing(ctypes.Structure):
     _fields_ = [("transport_ms", ctypes.c_float), ("pipeline_ms", ctypes.c_float), ("photons", ctypes.c_int64),
                 ("grid", ctypes.c_int32), ("block", ctypes.c_int32), ("chunk", ctypes.c_int32),
-                ("refill", ctypes.c_int32), ("prf_window", ctypes.c_int32)]
+                ("refill", ctypes.c_int32), ("prf_window", ctypes.c_int32), ("fresnel_batch", ctypes.c_int32)]
 
 
 class Events(ctypes.Structure):

@@ -322,6 +322,7 @@ fd2::TransportArgs transport_args(fd2_ctx *c)
     a.run_tag = reinterpret_cast<const uint32_t *>(c->d_flags + 1);
     a.chunk = c->cfg.chunk;
     a.refill = c->cfg.refill;
+    a.fresnel_batch = c->cfg.fresnel;
     a.window = c->cfg.window;
     a.win_x0 = c->win_x0;
     a.win_y0 = c->win_y0;
@@ -404,6 +405,7 @@ fd2_status set_config(fd2_ctx *c, const fd2::TransportConfig &cfg)
     k.ctas_per_sm = std::min(std::max(k.ctas_per_sm, 1), 32);
     k.chunk = std::min(std::max(k.chunk, 1), 4096);
     k.refill = std::min(std::max(k.refill, 1), 32);
+    k.fresnel = std::min(std::max(k.fresnel, 1), 32);
     const int window = c->cfg.window;
     c->cfg = k;
     c->cfg.window = window;
@@ -462,14 +464,17 @@ bool tune_cache_lookup(const fd2_ctx *c, fd2::TransportConfig *out)
     bool found = false;
     while (std::fgets(line, sizeof line, f)) {
         char k[512];
-        int b, s, ch, r;
-        if (std::sscanf(line, " \"%511[^\"]\": {\"block\": %d, \"ctas_per_sm\": %d, \"chunk\": %d, \"refill\": %d", k, &b,
-                        &s, &ch, &r) == 5 &&
+        int b, s, ch, r, fr;
+        if (std::sscanf(line,
+                        " \"%511[^\"]\": {\"block\": %d, \"ctas_per_sm\": %d, \"chunk\": %d, \"refill\": %d, "
+                        "\"fresnel\": %d",
+                        k, &b, &s, &ch, &r, &fr) == 6 &&
             key == k) {
             out->block = b;
             out->ctas_per_sm = s;
             out->chunk = ch;
             out->refill = r;
+            out->fresnel = fr;
             found = true;
         }
     }
@@ -495,8 +500,9 @@ void tune_cache_store(const fd2_ctx *c)
         std::fclose(f);
     }
     char b[1024];
-    std::snprintf(b, sizeof b, "  \"%s\": {\"block\": %d, \"ctas_per_sm\": %d, \"chunk\": %d, \"refill\": %d}",
-                  key.c_str(), c->cfg.block, c->cfg.ctas_per_sm, c->cfg.chunk, c->cfg.refill);
+    std::snprintf(b, sizeof b,
+                  "  \"%s\": {\"block\": %d, \"ctas_per_sm\": %d, \"chunk\": %d, \"refill\": %d, \"fresnel\": %d}",
+                  key.c_str(), c->cfg.block, c->cfg.ctas_per_sm, c->cfg.chunk, c->cfg.refill, c->cfg.fresnel);
     keep.push_back(b);
     if (FILE *f = std::fopen(c->opt.tune_cache, "w")) {
         std::fprintf(f, "{\n");
@@ -606,7 +612,8 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     cfg.block = c->opt.block_size > 0 ? c->opt.block_size : 256;
     cfg.ctas_per_sm = c->opt.ctas_per_sm > 0 ? c->opt.ctas_per_sm : 2;
     cfg.chunk = c->opt.chunk > 0 ? c->opt.chunk : 32;
-    cfg.refill = c->opt.refill > 0 ? c->opt.refill : 1;
+    cfg.refill = c->opt.refill > 0 ? c->opt.refill : 8;
+    cfg.fresnel = c->opt.fresnel_batch > 0 ? c->opt.fresnel_batch : 8;
     if ((st = set_config(c, cfg)) != FD2_OK) return bail(st);
     *out = c;
     return FD2_OK;
@@ -993,6 +1000,7 @@ fd2_status fd2_get_timing(fd2_ctx *c, fd2_timing *out)
     out->chunk = c->cfg.chunk;
     out->refill = c->cfg.refill;
     out->prf_window = c->cfg.window;
+    out->fresnel_batch = c->cfg.fresnel;
     return FD2_OK;
 }
 
@@ -1117,14 +1125,20 @@ fd2_status fd2_autotune(fd2_ctx *c, int32_t budget_runs)
     const std::vector<int> blocks = {128, 256, 384, 512};
     const std::vector<int> ctas = {1, 2, 3, 4};
     const std::vector<int> chunks = {8, 16, 32, 64, 128};
-    const std::vector<int> refills = {1, 2, 4, 8};
+    const std::vector<int> refills = {1, 4, 8, 16};
+    const std::vector<int> fresnels = {1, 4, 8, 16};
     for (int pass = 0; pass < 2; ++pass) {
-        for (int knob = 0; knob < 4; ++knob) {
-            const std::vector<int> &vals = knob == 0 ? blocks : knob == 1 ? ctas : knob == 2 ? chunks : refills;
+        for (int knob = 0; knob < 5; ++knob) {
+            const std::vector<int> &vals =
+                knob == 0 ? blocks : knob == 1 ? ctas : knob == 2 ? chunks : knob == 3 ? refills : fresnels;
             for (int v : vals) {
                 if (budget_runs > 0 && runs >= budget_runs) break;
                 fd2::TransportConfig k = best;
-                int &slot = knob == 0 ? k.block : knob == 1 ? k.ctas_per_sm : knob == 2 ? k.chunk : k.refill;
+                int &slot = knob == 0 ? k.block
+                            : knob == 1 ? k.ctas_per_sm
+                            : knob == 2 ? k.chunk
+                            : knob == 3 ? k.refill
+                                        : k.fresnel;
                 if (slot == v) continue;
                 slot = v;
                 // the CTA's shared memory must fit ctas_per_sm times

@@ -67,6 +67,10 @@ __device__ __forceinline__ float u01(uint32_t r)
 
 constexpr int kURing = 16;  // uniforms buffered per lane
 
+// Internal step result: the photon waits at a column wall for the Fresnel
+// part of its surface interaction (not a fate).
+constexpr int kNeedsFresnel = 100;
+
 // Warp-uniform part of a Philox stream: round keys (from the run seed) and
 // the run counter.
 struct RngKey {
@@ -434,9 +438,13 @@ struct Walker {
         return kCapped;
     }
 
-    // Interaction with a surface (boundary_analysis).
+    // Interaction with a surface (boundary_analysis), first part: the top
+    // surface and columnar crosstalk.  Returns a fate, kAlive, or
+    // kNeedsFresnel when the photon meets the column wall without crosstalk;
+    // the Fresnel part (surface_fresnel) can then run later, from the photon
+    // state alone.
     template <class G>
-    __device__ __forceinline__ int surface(const G &g)
+    __device__ __forceinline__ int surface_entry(const G &g)
     {
         if (at_top(g)) {
             if (g.top_absfrac > 0.0f && u() < g.top_absfrac) return kAbsTop;
@@ -454,18 +462,26 @@ struct Walker {
         if (pz <= g.half && pz >= g.cct_band_lo) cct = 1.0f;
         else if (pz < g.cct_band_lo && pz >= 0.0f) cct = fmaf(pz, g.cct_k_hi, 0.5f);
         else if (pz < 0.0f && pz >= -g.half) cct = fmaf(pz + g.half, g.cct_k_lo, 1.0f);
-        const bool cross = u() < cct;
+        if (!(u() < cct)) return kNeedsFresnel;
+        const int f = leave_column(g, true);
+        if (f != kAlive) return f;
+        xc = fmaf(-g.R, nx, px);
+        yc = fmaf(-g.R, ny, py);
+        return kAlive;
+    }
 
+    // Second part: Fresnel reflection / refraction on the rough wall, with
+    // hops between columns until the photon is back inside a column.
+    template <class G>
+    __device__ __forceinline__ int surface_fresnel(const G &g)
+    {
         bool outside = false;
         int tries_theta = 0, tries_normal = 0, reperturbs = 0, smooth = 0;
         float pr = __int_as_float(0x7fc00000);  // 0/0 until a rule sets it
         float st = 0.0f, ct = 1.0f;            // sin, cos of the last refraction angle
         float kx = 0, ky = 0, kz = 0, kdx = 0, kdy = 0, kdz = 0;
-        enum { kLeave, kNewSurface, kRestore, kIncidence, kDone } stage = cross ? kLeave : kNewSurface;
+        enum { kLeave, kNewSurface, kRestore, kIncidence } stage = kNewSurface;
         int fate = kAlive;
-        // The column change (kLeave) closes the loop body, so crosstalk lanes
-        // and lanes that refracted out of the column in this pass run
-        // leave_column -- the costly part -- together.
         for (int loop = 0; loop < kMaxSurfaceLoops; ++loop) {
             top_up();
             if (stage == kNewSurface) {
@@ -563,29 +579,23 @@ struct Walker {
                     stage = kLeave;
                 }
             }
-            // kLeave: change column (crosstalk, or a hop between columns)
-            const bool xt = cross && !outside;
-            const int f = leave_column(g, xt);
+            // kLeave: hop between columns
+            const int f = leave_column(g, false);
             if (f != kAlive) {
                 fate = f;
-                break;
-            }
-            if (xt) {
-                xc = fmaf(-g.R, nx, px);
-                yc = fmaf(-g.R, ny, py);
                 break;
             }
             outside = true;
             stage = kNewSurface;
             if (loop + 1 == kMaxSurfaceLoops) fate = kCapped;
         }
-        (void)kDone;
         return fate;
     }
 
     // One transport step (the body of the reference's step function algo):
-    // flight, sensor, trapped-photon restart, or a surface interaction.
-    // Returns the photon's fate, kAlive while it is in flight.
+    // flight, sensor, trapped-photon restart, or a surface interaction up to
+    // the Fresnel part.  Returns the photon's fate, kAlive while it is in
+    // flight, or kNeedsFresnel (run surface_fresnel next).
     template <class G>
     __device__ __forceinline__ int step(const G &g)
     {
@@ -611,7 +621,7 @@ struct Walker {
             return kAlive;
         }
         if (++rebound > kMaxBoundaryCalls) return kCapped;
-        return surface(g);
+        return surface_entry(g);
     }
 };
 

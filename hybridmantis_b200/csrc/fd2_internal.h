@@ -16,6 +16,7 @@ struct TransportConfig {
     int chunk = 32;      // photons per work-queue chunk
     int refill = 1;      // idle lanes that trigger a warp refill
     int window = 0;      // shared-memory PRF window edge (0 = off)
+    int fresnel = 8;     // parked lanes that trigger the warp's Fresnel pass
 };
 
 struct TransportArgs {
@@ -40,6 +41,7 @@ struct TransportArgs {
     const uint32_t *run_tag;     // device counter: runs since submission
     int chunk;
     int refill;
+    int fresnel_batch;           // parked lanes before the Fresnel pass runs
     int window;                  // window edge (0 = off), applies to geometry 0
     int win_x0, win_y0;          // window origin in pixels
     const volatile int *abort_flag;

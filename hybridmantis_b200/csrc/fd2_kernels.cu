@@ -358,8 +358,9 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     const unsigned long long total_chunks = min(*a.n_chunks, (unsigned long long)a.chunk_capacity);
     int ring_len = 0, slot = 0, refills = 0;
     uint32_t used = 0;
-    bool exhausted = false, alive = false;
+    bool exhausted = false, alive = false, parked = false;
     const unsigned refill_min = (unsigned)a.refill;
+    const unsigned fresnel_min = (unsigned)max(a.fresnel_batch, 1);
 
     __shared__ RngKey s_key;
     if (threadIdx.x < 20) s_key.rk[threadIdx.x] = a.round_keys[threadIdx.x];
@@ -441,9 +442,28 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             continue;
         }
 
-        // ---- one transport step per live lane
+        // ---- one transport step per live lane; a lane whose photon meets a
+        // column wall without crosstalk parks it there, and the warp runs the
+        // Fresnel part for the parked lanes together once `fresnel_batch` of
+        // them wait (or nothing else runs)
         int fate = kAlive;
-        if (alive) fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
+        if (alive && !parked) {
+            fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
+            if (fate == kNeedsFresnel) {
+                parked = true;
+                fate = kAlive;
+            }
+        }
+        const unsigned waiting = __ballot_sync(kFull, parked);
+        if (waiting) {
+            const unsigned busy = __ballot_sync(kFull, alive && !parked && fate == kAlive);
+            if ((unsigned)__popc(waiting) >= fresnel_min || busy == 0) {
+                if (parked) {
+                    fate = kMulti ? w.surface_fresnel(s_geom[geom]) : w.surface_fresnel(a.g0);
+                    parked = false;
+                }
+            }
+        }
 
         // ---- warp-aggregated tallies of the photons that ended
         const unsigned ended = __ballot_sync(kFull, fate != kAlive);

@@ -161,7 +161,7 @@ class OpticalTransport:
     def __init__(self, params: Params, *, device: int = 0, count_mode: int = COUNT_POISSON, seed: int | None = None,
                  block_size: int = 0, ctas_per_sm: int = 0, chunk: int = 0, refill: int = 0, prf_window: int = -1,
                  use_graph: bool = True, wait_timeout_s: float = 0.0, max_photons_per_event: int = 900000,
-                 tune_cache: str | None = None, event_base: int = 0):
+                 tune_cache: str | None = None, event_base: int = 0, fresnel_batch: int = 0):
         lib = load()
         self._lib = lib
         opt = Options()
@@ -176,6 +176,7 @@ class OpticalTransport:
         opt.wait_timeout_s = wait_timeout_s
         opt.max_photons_per_event = max_photons_per_event
         opt.event_base = event_base
+        opt.fresnel_batch = fresnel_batch
         self._tune_cache = tune_cache.encode() if tune_cache else None
         opt.tune_cache = self._tune_cache
         self.params = params

@@ -22,11 +22,12 @@ def main():
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--refill", type=int, default=0)
     ap.add_argument("--window", type=int, default=-1)
+    ap.add_argument("--fresnel", type=int, default=0)
     a = ap.parse_args()
     es = fd.synth_events(a.config, a.xrays, a.seed)
     x, y, z = es.to_cm()
     with fd.OpticalTransport(es.params, block_size=a.block, ctas_per_sm=a.ctas, chunk=a.chunk, refill=a.refill,
-                             prf_window=a.window) as t:
+                             prf_window=a.window, fresnel_batch=a.fresnel) as t:
         t.submit_events(x, y, z, es.e_ev.astype(np.float64), es.hist)
         out = []
         for _ in range(a.runs):
@@ -35,7 +36,8 @@ def main():
             out.append({"transport_ms": tm["transport_ms"], "photons": tm["photons"],
                         "photons_per_s": tm["photons"] / (tm["transport_ms"] * 1e-3)})
         print(json.dumps({"events": es.n, "runs": out, "launch": {k: tm[k] for k in
-                                                                 ("grid", "block", "chunk", "refill", "prf_window")}}))
+                                                                 ("grid", "block", "chunk", "refill", "prf_window",
+                                                                                  "fresnel_batch")}}))
 
 
 if __name__ == "__main__":

@@ -123,6 +123,9 @@ typedef struct fd2_options {
     int64_t event_base;            /* global index of the first submitted event: a
                                       shard of a larger stream draws the same
                                       random numbers as in the unsharded run     */
+    int32_t fresnel_batch;         /* lanes parked at a column wall before the warp
+                                      runs their Fresnel interaction; 0 = tuned   */
+    int32_t reserved;
 } fd2_options;
 
 typedef struct fd2_counters {
@@ -143,7 +146,7 @@ typedef struct fd2_timing {
     float transport_ms; /* persistent transport kernel, last run        */
     float pipeline_ms;  /* count + queue + transport + PHS, last run     */
     int64_t photons;    /* photons transported in the last run          */
-    int32_t grid, block, chunk, refill, prf_window;
+    int32_t grid, block, chunk, refill, prf_window, fresnel_batch;
 } fd2_timing;
 
 typedef struct fd2_ctx fd2_ctx;
