@@ -108,7 +108,7 @@ EXPORTED = [
     "fd2_reset_tallies", "fd2_get_counters", "fd2_get_prf_dims", "fd2_get_prf",
     "fd2_get_detected_per_primary", "fd2_get_photon_counts", "fd2_get_phs", "fd2_get_phs_stats",
     "fd2_get_timing", "fd2_get_stream", "fd2_write_outputs", "fd2_write_output_files", "fd2_replay",
-    "fd2_autotune",
+    "fd2_autotune", "fd2_transport_noalloc",
     "fd2_synth_events", "fd2_free_events", "fd2_read_events_text", "fd2_write_events_text",
     "fd2_read_events_binary", "fd2_write_events_binary",
     "gpuoptical_", "cpuoptical_", "fd2_compat_status",
@@ -156,6 +156,8 @@ def load():
                                                   ctypes.c_int32, ctypes.c_double, ctypes.c_char_p, ctypes.c_char_p]),
         "fd2_replay": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, vp, vp, vp, vp]),
         "fd2_autotune": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "fd2_transport_noalloc": (ctypes.c_int, [P(Geometry), vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int32,
+                                                 ctypes.c_uint64, vp, vp, vp, vp]),
         "fd2_synth_events": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, P(Events)]),
         "fd2_free_events": (None, [P(Events)]),
         "fd2_read_events_text": (ctypes.c_int, [ctypes.c_char_p, P(Events)]),

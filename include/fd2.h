@@ -224,6 +224,28 @@ FD2_API fd2_status fd2_replay(fd2_ctx *ctx, int32_t mode, int32_t seed_input,
                               int64_t event_index_base, int8_t *fate, int32_t *pix,
                               int32_t *seeds, int32_t *steps);
 
+/* Transport without allocating, for callers that cannot allocate device
+ * memory (code running inside another framework's memory pool, or that may
+ * not change the device's memory footprint).  No counterpart in the
+ * reference.  All pointers are device pointers; events in micrometres with
+ * 1-based histories (<= num_hist) and given photon counts; tallies are added
+ * into prf (xdim*ydim u64, [ii*ydim + jj]), per_primary (num_hist int32,
+ * index hist-1) and counters (9 u64: unused, detected, abs_top, abs_bulk,
+ * lost, outofcol, theta1, capped, detected in the PRF).  At most 262144
+ * events and 2097152 work-queue chunks of 256 photons per call; larger
+ * inputs return FD2_ERR_INVALID_ARGUMENT.  The work queue lives in one
+ * fixed ~24 MiB __device__ array that every GPU loading the library holds
+ * until exit; the first call on a device looks up its address (make it
+ * before any stream capture on that device).  Calls share that array:
+ * calls that overlap on the GPU race, so serialise them.  Synchronises
+ * `stream` (a cudaStream_t, NULL = legacy default stream) before returning.
+ * Same random streams as fd2_run's first run with seed `seed`, so the
+ * tallies equal the context API's for the same events. */
+FD2_API fd2_status fd2_transport_noalloc(const fd2_geometry *geometry, const float *x_um, const float *y_um,
+                                         const float *z_um, const int32_t *hist, const int32_t *nphot, int64_t n,
+                                         int32_t num_hist, uint64_t seed, uint64_t *prf, int32_t *per_primary,
+                                         uint64_t *counters, void *stream);
+
 /* Autotuner: times transport configurations on the resident events and
  * keeps the fastest (cached in options.tune_cache when set). */
 FD2_API fd2_status fd2_autotune(fd2_ctx *ctx, int32_t budget_runs);
