@@ -13,6 +13,9 @@ photon counts ~ Poisson(E * 54/keV) sampled on the GPU each step.
   roofline  the transport kernel against the FP32 issue roofline
   cpu_baseline  the reference's own C transport (oracle/_ref, gcc -O2,
           all host cores) on a bounded sample of the same stream
+  reference_gpu the reference's own CUDA kernel `algo` (oracle/_ref,
+          compiled for sm_100a with its own flags) on the same events and
+          photon counts, one launch of its 18000 x 128 grid
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU: one rank per GPU (torchrun); each rank transports its own x-ray
@@ -71,6 +74,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-ref-gpu", action="store_true")
     return ap.parse_args()
 
 
@@ -139,6 +143,28 @@ class CpuReference:
 
     def close(self):
         self.pool.shutdown()
+
+
+# DRAM bytes per photon of the transport kernel: dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture (3,348,480 B for 4,690,971 photons
+# of the config-1 stream, 2,000 x-rays); the traffic is one event record per
+# chunk and grows in proportion to the photons.
+TRANSPORT_DRAM_BYTES_PER_PHOTON = 3348480.0 / 4690971.0
+
+
+def reference_gpu(es, nphot, device):
+    """One launch of the reference's CUDA kernel over the step's events."""
+    from oracle import pyoracle as po
+    if not po.ref_cuda_available():
+        return None
+    r = po.run_ref_cuda(_oracle_geometry(es.params), es.x_um.astype(np.float64), es.y_um.astype(np.float64),
+                        es.z_um.astype(np.float64), es.hist, nphot, num_hist=int(es.params.num_hist), grid=18000,
+                        device=device)
+    ms = r.extra["kernel_ms"]
+    photons = int(np.sum(nphot))
+    return {"value": photons / (ms / 1e3), "unit": "photons/s", "kernel_ms": ms, "photons": photons,
+            "kind": "reference CUDA kernel algo (main/kernel_cuda_c_ver1_0.cu, -DUSING_CUDA -use_fast_math -O3) "
+                    "compiled for sm_100a, GRIDSIZE 18000 x BLOCKSIZE 128, events resident, CUDA-event timed"}
 
 
 def work_per_photon(es, nphot, n_events=300):
@@ -326,7 +352,10 @@ def run_ours(a, rank, world, local_rank):
         avg_kern_s = float(np.mean(kern_ms)) / 1e3
         achieved = photons_per_launch * wpp / avg_kern_s / 1e12
         roofline = {"bound": "fp32-issue", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                    "frac": achieved / peak_tflops, "traffic": None,
+                    "frac": achieved / peak_tflops,
+                    "traffic": TRANSPORT_DRAM_BYTES_PER_PHOTON * photons_per_launch,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 2,000-x-ray capture, "
+                                      "scaled by photons",
                     "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 (FMA) x {sm_max:.0f} MHz "
                                    f"(sm_max_mhz of MEASURED_PEAKS.json; the file has no FP32 entry)",
                     "work_per_photon_fp32_ops": wpp, "kernel_ms_per_launch": avg_kern_s * 1e3,
@@ -339,6 +368,9 @@ def run_ours(a, rank, world, local_rank):
             cpu = {"value": rate, "unit": "photons/s", "cores": ref.cores, "kind": "reference",
                    "sample": f"first {nev} events ({ph} photons) of the same stream and the same photon counts, "
                              f"reference C transport (gcc -O2), {ref.cores} processes, {dt:.1f} s"}
+        ref_gpu = None
+        if not a.no_ref_gpu and world == 1:
+            ref_gpu = reference_gpu(es, nphot, local_rank)
         clocks = clk.summary()
         out = {
             "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": a.steps,
@@ -352,9 +384,11 @@ def run_ours(a, rank, world, local_rank):
                                                            "fresnel_batch")}},
             "e2e": {"value": e2e_photons / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": a.steps * 9,
+            # per step: count, scan_tiles, scan_sums, scan_add, fill_chunks, transport, phs, bump
+            "gpu_launches": a.steps * 8,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "clocks": clocks,
             "results": {"phs_mean": stats["mean"], "swank": stats["swank"],
                         "fates_per_photon": {k: cnt[k] / max(cnt["generated"], 1) for k in

@@ -5,7 +5,9 @@ bench.py's CPU-baseline leg.  The product package never imports this.
 
 ``run_oracle`` calls the C restatement (oracle/fd2_oracle.c); ``run_ref``
 calls the reference's own C transport compiled in place (oracle/_ref, built
-by oracle/Makefile from main/kernel_cuda_c_ver1_0.cu).
+by oracle/Makefile from main/kernel_cuda_c_ver1_0.cu); ``run_ref_cuda``
+launches the reference's own CUDA kernel from the same file, compiled for
+sm_100a (the GPU baseline; needs a GPU).
 """
 from __future__ import annotations
 
@@ -20,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libfd2oracle.so")
 REF_SO = {"O0": os.path.join(HERE, "_ref", "libfd2ref_O0.so"),
           "O2": os.path.join(HERE, "_ref", "libfd2ref_O2.so")}
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libfd2refcuda.so")
 
 FATE_NAMES = {0: "none", 1: "detect", 2: "abs_top", 3: "abs_bulk", 4: "lost",
               5: "outofcol", 6: "theta1"}
@@ -222,3 +225,38 @@ def phs(per_primary, min_photons, max_photons, num_bins):
     if rc != 0:
         raise ValueError("PHS bin width is zero")
     return h
+
+
+def ref_cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_SO)
+
+
+def run_ref_cuda(g: Geometry, x, y, z, hist, nphot, num_hist: int, grid: int = 18000,
+                 device: int = 0) -> RunResult:
+    """Launch the reference's CUDA kernel once over the events (inputs in um).
+
+    ``grid`` = 18000 is the reference's fixed launch (cuda:82); 0 = just enough
+    blocks of 128 threads.  ``extra["kernel_ms"]`` is the CUDA-event time of
+    the launch.  Counters: generated, detect, abs_top, abs_bulk, lost,
+    outofcol, theta1.
+    """
+    lib = _load(REF_CUDA_SO)
+    x, y, z, hist, nphot = _events(x, y, z, hist, nphot)
+    n = len(x)
+    xdim, ydim = g.xdim, g.ydim
+    image = np.zeros(xdim * ydim, np.uint64)
+    prim = np.zeros(num_hist, np.int32)
+    cnt = np.zeros(7, np.uint64)
+    ms = ctypes.c_float(0.0)
+    err = ctypes.c_int(0)
+    rg = _RGeom((ctypes.c_float * 16)(*g.floats()), ctypes.c_int(g.pixel))
+    lib.fd2refcu_run.restype = ctypes.c_int
+    rc = lib.fd2refcu_run(ctypes.c_int(device), ctypes.byref(rg), ctypes.c_int64(n),
+                          _ptr(x, ctypes.c_double), _ptr(y, ctypes.c_double), _ptr(z, ctypes.c_double),
+                          _ptr(hist, ctypes.c_int32), _ptr(nphot, ctypes.c_int32), ctypes.c_int(num_hist),
+                          ctypes.c_int(grid), ctypes.c_int(xdim), ctypes.c_int(ydim),
+                          _ptr(image, ctypes.c_uint64), _ptr(prim, ctypes.c_int32), _ptr(cnt, ctypes.c_uint64),
+                          ctypes.byref(ms), ctypes.byref(err))
+    if rc != 0:
+        raise RuntimeError(f"fd2refcu_run returned {rc} (CUDA error {err.value})")
+    return RunResult(image.reshape(xdim, ydim), prim, cnt, extra={"kernel_ms": float(ms.value)})
