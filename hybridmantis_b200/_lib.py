@@ -64,7 +64,7 @@ class Options(ctypes.Structure):
         ("ctas_per_sm", ctypes.c_int32), ("chunk", ctypes.c_int32), ("refill", ctypes.c_int32),
         ("prf_window", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("wait_timeout_s", ctypes.c_double),
         ("tune_cache", ctypes.c_char_p), ("event_base", ctypes.c_int64), ("fresnel_batch", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("radial_bins", ctypes.c_int32), ("radial_max_um", ctypes.c_double),
     ]
 
 
@@ -98,20 +98,46 @@ class Events(ctypes.Structure):
     ]
 
 
+class SgConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("hidden", ctypes.c_int32), ("radial_bins", ctypes.c_int32),
+                ("radial_max_um", ctypes.c_double), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("adam_eps", ctypes.c_float),
+                ("radial_weight", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+
+class SgHull(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_float * 8), ("hi", ctypes.c_float * 8)]
+
+
+class SgStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ["events", "surrogate_events", "mc_events", "audit_events",
+                                              "surrogate_photons", "surrogate_detected"]] + \
+               [(n, ctypes.c_double) for n in ["audit_mc_detected", "audit_sg_expected", "audit_photons",
+                                               "audit_z", "audit_radial_l1"]] + \
+               [(n, ctypes.c_float) for n in ["sg_ms", "mc_ms", "audit_ms", "total_ms"]]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _lib = None
 
-# Every symbol include/fd2.h and include/fd2_compat.h declare.
+# Every symbol include/*.h declare.
 EXPORTED = [
     "fd2_status_string", "fd2_default_options", "fd2_parse_input_file", "fd2_params_fill_tags",
     "fd2_params_to_geometry", "fd2_prf_dims", "fd2_create", "fd2_destroy", "fd2_last_error",
     "fd2_set_geometries", "fd2_submit_events", "fd2_submit_events_um", "fd2_run", "fd2_wait",
     "fd2_reset_tallies", "fd2_get_counters", "fd2_get_prf_dims", "fd2_get_prf",
-    "fd2_get_detected_per_primary", "fd2_get_photon_counts", "fd2_get_phs", "fd2_get_phs_stats",
+    "fd2_get_detected_per_primary", "fd2_get_radial", "fd2_get_photon_counts", "fd2_get_phs", "fd2_get_phs_stats",
     "fd2_get_timing", "fd2_get_stream", "fd2_write_outputs", "fd2_write_output_files", "fd2_replay",
     "fd2_autotune", "fd2_transport_noalloc",
     "fd2_synth_events", "fd2_free_events", "fd2_read_events_text", "fd2_write_events_text",
     "fd2_read_events_binary", "fd2_write_events_binary",
-    "gpuoptical_", "cpuoptical_", "fd2_compat_status",
+    "gpuoptical_", "cpuoptical_", "gpuoptlb_", "cpuoptlb_", "fd2_compat_status",
+    "fd2_sg_default_config", "fd2_sg_create", "fd2_sg_destroy", "fd2_sg_last_error", "fd2_sg_set_data",
+    "fd2_sg_train", "fd2_sg_eval", "fd2_sg_num_params", "fd2_sg_get_params", "fd2_sg_set_params",
+    "fd2_sg_get_hull", "fd2_sg_set_hull", "fd2_sg_save", "fd2_sg_load", "fd2_sg_loss_grad", "fd2_sg_predict",
+    "fd2_sg_run",
 ]
 
 
@@ -146,6 +172,7 @@ def load():
         "fd2_get_prf_dims": (ctypes.c_int, [vp, ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]),
         "fd2_get_prf": (ctypes.c_int, [vp, ctypes.c_int32, vp, ctypes.c_int64]),
         "fd2_get_detected_per_primary": (ctypes.c_int, [vp, vp, ctypes.c_int64]),
+        "fd2_get_radial": (ctypes.c_int, [vp, vp, ctypes.c_int64]),
         "fd2_get_photon_counts": (ctypes.c_int, [vp, vp, ctypes.c_int64]),
         "fd2_get_phs": (ctypes.c_int, [vp, ctypes.c_int32, vp, ctypes.c_int32]),
         "fd2_get_phs_stats": (ctypes.c_int, [vp, ctypes.c_int32, P(PhsStats)]),
@@ -165,6 +192,23 @@ def load():
         "fd2_read_events_binary": (ctypes.c_int, [ctypes.c_char_p, P(Events)]),
         "fd2_write_events_binary": (ctypes.c_int, [ctypes.c_char_p, P(Events)]),
         "fd2_compat_status": (ctypes.c_int, []),
+        "fd2_sg_default_config": (None, [P(SgConfig)]),
+        "fd2_sg_create": (ctypes.c_int, [P(SgConfig), P(vp)]),
+        "fd2_sg_destroy": (None, [vp]),
+        "fd2_sg_last_error": (ctypes.c_char_p, [vp]),
+        "fd2_sg_set_data": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64]),
+        "fd2_sg_train": (ctypes.c_int, [vp, ctypes.c_int32, P(ctypes.c_float), P(ctypes.c_float)]),
+        "fd2_sg_eval": (ctypes.c_int, [vp, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)]),
+        "fd2_sg_num_params": (ctypes.c_int64, [vp]),
+        "fd2_sg_get_params": (ctypes.c_int, [vp, vp, ctypes.c_int64]),
+        "fd2_sg_set_params": (ctypes.c_int, [vp, vp, ctypes.c_int64]),
+        "fd2_sg_get_hull": (ctypes.c_int, [vp, P(SgHull)]),
+        "fd2_sg_set_hull": (ctypes.c_int, [vp, P(SgHull)]),
+        "fd2_sg_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "fd2_sg_load": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "fd2_sg_loss_grad": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int32, P(ctypes.c_float), vp]),
+        "fd2_sg_predict": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp]),
+        "fd2_sg_run": (ctypes.c_int, [vp, vp, ctypes.c_double, P(SgStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -23,70 +23,9 @@
 
 #include "fd2.h"
 #include "fd2_host.h"
+#include "fd2_ctx.h"
 #include "fd2_internal.h"
 
-using fd2::DevGeom;
-
-struct fd2_ctx {
-    fd2_params params{};
-    fd2_options opt{};
-    int device = 0, sm_count = 0;
-    std::string device_name, last_error;
-    cudaStream_t stream = nullptr;
-
-    // geometries
-    std::vector<fd2_geometry> geoms;
-    std::vector<DevGeom> dgeoms;
-    int64_t prf_total = 0;
-    DevGeom *d_geoms = nullptr;
-
-    // events
-    int64_t n_events = 0, cap_events = 0;
-    float4 *d_ev_pos = nullptr;
-    double *d_ev_e = nullptr, *d_ev_xyz = nullptr;
-    uint16_t *d_ev_geom = nullptr;
-    bool has_geom = false;
-    int32_t *d_given_n = nullptr, *d_ev_n = nullptr;
-    uint32_t *d_ev_nchunks = nullptr;
-    unsigned long long *d_chunk_off = nullptr, *d_block_sums = nullptr;
-    uint2 *d_chunks = nullptr;
-    int64_t chunk_cap = 0;
-    double mu_total = 0.0;
-    bool counts_ready = false;
-    std::vector<double> hist_per_geom;
-
-    // staging
-    void *d_stage = nullptr;
-    size_t d_stage_bytes = 0;
-    void *h_stage = nullptr;
-    size_t h_stage_bytes = 0;
-
-    // per-run device scalars: [0] chunks, [1] queue head, [2] photon total, [3..3+G) photons per geometry
-    unsigned long long *d_scalars = nullptr;
-    unsigned long long *d_gen_total = nullptr;  // photons per geometry, counted runs (transport passes)
-    int *d_flags = nullptr;  // [0] status bits, [1] run counter
-
-    // tallies
-    int32_t n_prim = 0;
-    unsigned long long *d_prf = nullptr, *d_counters = nullptr, *d_dropped = nullptr;
-    int32_t *d_per_primary = nullptr, *d_prim_geom = nullptr, *d_phs = nullptr;
-    double *d_distance = nullptr, *d_moments = nullptr;
-
-    // abort flag in mapped host memory
-    int *h_abort = nullptr, *d_abort = nullptr;
-
-    cudaEvent_t ev_start = nullptr, ev_t0 = nullptr, ev_t1 = nullptr, ev_end = nullptr;
-    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-    bool graph_valid = false;
-    bool run_pending = false, ran_once = false;
-    fd2::TransportConfig cfg;
-    int win_x0 = 0, win_y0 = 0;
-    int64_t last_photons = 0;
-
-    // float-libm corrections of the reference-arithmetic replay
-    uint32_t *d_libm = nullptr;
-    uint32_t n_acos = 0, n_asin = 0;
-};
 
 namespace {
 
@@ -273,6 +212,7 @@ void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *g
     const DevGeom &g = c->dgeoms[0];
     int w = c->opt.prf_window;
     if (w < 0) w = 128;
+    if (c->d_radial) w = 0;  // label mode tallies no PRF image
     if (w > g.xdim) w = g.xdim;
     if (w > g.ydim) w = g.ydim;
     if (w > 176) w = 176;  // fits beside the rings in shared memory
@@ -328,6 +268,9 @@ fd2::TransportArgs transport_args(fd2_ctx *c)
     a.win_y0 = c->win_y0;
     a.abort_flag = c->d_abort;
     a.status = c->d_flags;
+    a.radial = c->d_radial;
+    a.radial_bins = c->d_radial ? c->opt.radial_bins : 0;
+    a.radial_inv_width = c->d_radial ? (float)(c->opt.radial_bins / c->opt.radial_max_um) : 0.0f;
     return a;
 }
 
@@ -514,6 +457,19 @@ void tune_cache_store(const fd2_ctx *c)
 
 }  // namespace
 
+namespace fd2 {
+namespace api {
+
+cudaError_t count_pass(fd2_ctx *c, bool for_transport) { return ::count_pass(c, for_transport); }
+cudaError_t enqueue_segment(fd2_ctx *c, int seg) { return ::enqueue_segment(c, seg); }
+TransportArgs transport_args(fd2_ctx *c) { return ::transport_args(c); }
+fd2_status ensure_chunks(fd2_ctx *c) { return ::ensure_chunks(c); }
+fd2_status check_status(fd2_ctx *c) { return ::check_status(c); }
+fd2_status fail(fd2_ctx *c, fd2_status s, const std::string &msg) { return ::fail(c, s, msg); }
+
+}  // namespace api
+}  // namespace fd2
+
 extern "C" {
 
 const char *fd2_status_string(fd2_status s)
@@ -553,6 +509,8 @@ void fd2_default_options(fd2_options *o)
     o->wait_timeout_s = 0.0;
     o->tune_cache = nullptr;
     o->event_base = 0;
+    o->radial_bins = 0;
+    o->radial_max_um = 200.0;
 }
 
 const char *fd2_last_error(const fd2_ctx *c) { return c ? c->last_error.c_str() : "no context"; }
@@ -569,7 +527,8 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     if (opt) c->opt = *opt;
     else fd2_default_options(&c->opt);
     if (c->opt.max_photons_per_event <= 0) c->opt.max_photons_per_event = 900000;
-    if (c->opt.event_base < 0) {
+    if (c->opt.event_base < 0 || c->opt.radial_bins < 0 || c->opt.radial_bins > 4096 ||
+        (c->opt.radial_bins > 0 && !(c->opt.radial_max_um > 0.0))) {
         delete c;
         return FD2_ERR_INVALID_ARGUMENT;
     }
@@ -606,6 +565,10 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     c->n_prim = p->num_hist;
     if (dalloc(&c->d_per_primary, (size_t)c->n_prim) != cudaSuccess || dalloc(&c->d_prim_geom, (size_t)c->n_prim) != cudaSuccess)
         return bail(FD2_ERR_OUT_OF_MEMORY);
+    if (c->opt.radial_bins > 0) {
+        c->radial_len = (int64_t)std::max(c->n_prim, 1) * (c->opt.radial_bins + 1);
+        if (dalloc(&c->d_radial, (size_t)c->radial_len) != cudaSuccess) return bail(FD2_ERR_OUT_OF_MEMORY);
+    }
     c->geoms.assign(1, g);
     if ((st = alloc_tallies(c)) != FD2_OK) return bail(st);
     fd2::TransportConfig cfg;
@@ -644,6 +607,7 @@ void fd2_destroy(fd2_ctx *c)
     dfree(c->d_counters);
     dfree(c->d_dropped);
     dfree(c->d_per_primary);
+    dfree(c->d_radial);
     dfree(c->d_prim_geom);
     dfree(c->d_phs);
     dfree(c->d_distance);
@@ -880,6 +844,7 @@ fd2_status fd2_reset_tallies(fd2_ctx *c)
     FD2_CUDA(c, cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * G * fd2::kCounterStride, c->stream));
     FD2_CUDA(c, cudaMemsetAsync(c->d_distance, 0, sizeof(double) * G, c->stream));
     FD2_CUDA(c, cudaMemsetAsync(c->d_per_primary, 0, sizeof(int32_t) * (size_t)std::max(c->n_prim, 1), c->stream));
+    if (c->d_radial) FD2_CUDA(c, cudaMemsetAsync(c->d_radial, 0, sizeof(uint32_t) * (size_t)c->radial_len, c->stream));
     FD2_CUDA(c, cudaMemsetAsync(c->d_prim_geom, 0, sizeof(int32_t) * (size_t)std::max(c->n_prim, 1), c->stream));
     FD2_CUDA(c, cudaMemsetAsync(c->d_phs, 0, sizeof(int32_t) * G * (size_t)std::max(c->params.num_bins, 1), c->stream));
     FD2_CUDA(c, cudaMemsetAsync(c->d_moments, 0, sizeof(double) * G * 3, c->stream));
@@ -941,6 +906,17 @@ fd2_status fd2_get_detected_per_primary(fd2_ctx *c, int32_t *counts, int64_t n)
     fd2_status st = fd2_wait(c);
     if (st != FD2_OK) return st;
     if (c->n_prim) FD2_CUDA(c, cudaMemcpy(counts, c->d_per_primary, sizeof(int32_t) * (size_t)c->n_prim, cudaMemcpyDeviceToHost));
+    return FD2_OK;
+}
+
+fd2_status fd2_get_radial(fd2_ctx *c, uint32_t *counts, int64_t n)
+{
+    if (!c) return FD2_ERR_INVALID_ARGUMENT;
+    if (!c->d_radial) return fail(c, FD2_ERR_STATE, "label mode is off (options.radial_bins = 0)");
+    if (!counts || n < c->radial_len) return fail(c, FD2_ERR_INVALID_ARGUMENT, "buffer too small");
+    fd2_status st = fd2_wait(c);
+    if (st != FD2_OK) return st;
+    FD2_CUDA(c, cudaMemcpy(counts, c->d_radial, sizeof(uint32_t) * (size_t)c->radial_len, cudaMemcpyDeviceToHost));
     return FD2_OK;
 }
 

@@ -1,6 +1,7 @@
 // fd2_compat.cpp -- gpuoptical_ / cpuoptical_ over the C ABI, with the
 // reference's Fortran COMMON-block data exchange (see include/fd2_compat.h).
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -133,6 +134,30 @@ void gpuoptical_(int *penctr, int *myfactGPU)
     }
     report(s, g_gpu, "gpuoptical_");
 }
+
+// Load-balancing probes of the _LB build: transport optical_ events
+// [0, *count) synchronously, add the results into the COMMON blocks and
+// return the seconds taken (gpuoptlb_, cuda_LB:108-280; cpuoptlb_,
+// c_LB:86-286).  Both run on the GPU.
+static void lb_probe(double *seconds, int *count, const char *where)
+{
+    if (!seconds || !count || !commons_present()) return report(FD2_ERR_STATE, nullptr, where);
+    const fd2_params p = params_from_common();
+    fd2_ctx *c = nullptr;
+    fd2_status s = fd2_create(&p, nullptr, &c);
+    const auto t0 = std::chrono::steady_clock::now();
+    if (s == FD2_OK) s = submit_range(c, 0, std::min(*count, FD2_GPUBUFSIZE));
+    if (s == FD2_OK) s = fd2_run(c);
+    if (s == FD2_OK) s = fd2_wait(c);
+    if (s == FD2_OK) s = accumulate_into_commons(c);
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    report(s, c, where);
+    fd2_destroy(c);
+}
+
+void gpuoptlb_(double *gptime, int *lbbuf) { lb_probe(gptime, lbbuf, "gpuoptlb_"); }
+
+void cpuoptlb_(double *cptime, int *cpubufsize) { lb_probe(cptime, cpubufsize, "cpuoptlb_"); }
 
 void cpuoptical_(int *gpusize)
 {

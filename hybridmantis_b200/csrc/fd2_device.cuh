@@ -9,9 +9,11 @@
 //   * every uniform comes from Philox keyed by the run seed at counter
 //     (block, photon-in-event, event, run), so a photon's walk does not
 //     depend on which lane runs it or when;
-//   * uniforms are generated four at a time into a 16-entry per-lane ring in
-//     shared memory at one convergent point per step, so the walk's draw
-//     sites are a shared-memory load, not an inlined Philox;
+//   * uniforms are generated four at a time into a 32-entry per-lane ring in
+//     shared memory, so the walk's draw sites are a shared-memory load, not
+//     an inlined Philox; whenever one lane of the warp must generate, every
+//     lane with room generates too, so the Philox rounds run with most of
+//     the warp instead of the few lanes whose rings happen to be low;
 //   * angle tests are made on cosines (acos(c) > 1.57 <=> c < cos 1.57) and
 //     the Fresnel coefficients use the cosine forms, so the walk needs no
 //     acos/asin/tan/pow; the refraction keeps the reference's formula
@@ -65,16 +67,18 @@ __device__ __forceinline__ float u01(uint32_t r)
     return __uint_as_float(0x3F800000u | (r >> 9)) - 0.99999994039535522461f;
 }
 
-constexpr int kURing = 16;  // uniforms buffered per lane
+constexpr int kURing = 32;     // uniforms buffered per lane
+constexpr int kURingLow = 12; // a lane at or below this level must generate
 
 // Internal step result: the photon waits at a column wall for the Fresnel
 // part of its surface interaction (not a fate).
 constexpr int kNeedsFresnel = 100;
 
-// Warp-uniform part of a Philox stream: round keys (from the run seed) and
-// the run counter.
+// Warp-uniform part of a Philox stream: the round keys of the run seed,
+// read where the kernel keeps them (its __grid_constant__ parameters, so
+// the rounds take them as constant-bank operands), and the run counter.
 struct RngKey {
-    uint32_t rk[20];
+    const uint32_t *rk;
     uint32_t run;
 };
 
@@ -129,26 +133,31 @@ struct Walker {
     uint32_t rebound;   // boundary interactions
     int ii, jj;         // detection pixel (-1: outside the PRF bounds)
     // Philox stream of the photon and the lane's uniform ring.  The ring is
-    // topped up to at least 13 uniforms at the start of every step, loop
-    // iteration and new-normal attempt; no segment between two top-ups draws
-    // more than 7, so a draw is a plain shared-memory load.  `underflow`
-    // records a draw from an empty ring (never expected; reported).
+    // topped up to at least kURingLow + 1 = 13 uniforms at the start of every
+    // step, loop iteration and new-normal attempt; no segment between two
+    // top-ups draws more than 7, so a draw is a plain shared-memory load.
+    // `underflow` records a draw from an empty ring (never expected;
+    // reported).  Generating ahead does not change the values a photon
+    // draws: its stream is consumed in counter order either way.
     float *ring;
     int stride;
     uint32_t head, tail, block, photon, event;
-    const RngKey *key;
+    RngKey key;
     bool underflow;
 
     __device__ __forceinline__ void top_up()
     {
+        const unsigned mask = __activemask();
 #pragma unroll 1
-        while (tail - head <= (uint32_t)(kURing - 4)) {
-            const uint4 r = philox4x32_10_rk(make_uint4(block++, photon, event, key->run), key->rk);
-            ring[((tail + 0) & (kURing - 1)) * stride] = u01(r.x);
-            ring[((tail + 1) & (kURing - 1)) * stride] = u01(r.y);
-            ring[((tail + 2) & (kURing - 1)) * stride] = u01(r.z);
-            ring[((tail + 3) & (kURing - 1)) * stride] = u01(r.w);
-            tail += 4;
+        while (__any_sync(mask, tail - head <= (uint32_t)kURingLow)) {
+            if (tail - head <= (uint32_t)(kURing - 4)) {
+                const uint4 r = philox4x32_10_rk(make_uint4(block++, photon, event, key.run), key.rk);
+                ring[((tail + 0) & (kURing - 1)) * stride] = u01(r.x);
+                ring[((tail + 1) & (kURing - 1)) * stride] = u01(r.y);
+                ring[((tail + 2) & (kURing - 1)) * stride] = u01(r.z);
+                ring[((tail + 3) & (kURing - 1)) * stride] = u01(r.w);
+                tail += 4;
+            }
         }
     }
     __device__ __forceinline__ float u()

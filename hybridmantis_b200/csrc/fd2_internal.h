@@ -46,6 +46,10 @@ struct TransportArgs {
     int win_x0, win_y0;          // window origin in pixels
     const volatile int *abort_flag;
     int *status;
+    // label mode: per-history radial histograms of detected photons
+    unsigned int *radial;        // [n_prim][radial_bins + 1], null = off
+    int radial_bins;
+    float radial_inv_width;      // bins per micrometre
 };
 
 // Device status bits (the `status` word).

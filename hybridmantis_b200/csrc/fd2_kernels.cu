@@ -329,8 +329,10 @@ struct SmemLayout {
 // pixels are aggregated across the warp before touching memory; the PRF
 // core of geometry 0 is tallied in a shared-memory window.  kMulti: the
 // geometry of each photon comes from the table in shared memory; otherwise
-// the single geometry is read from the kernel parameters.
-template <bool kMulti, int kMaxThreads, int kMinBlocks>
+// the single geometry is read from the kernel parameters.  kRadial (label
+// mode): a detected photon is binned by its distance from its event into
+// the history's radial histogram instead of the PRF image.
+template <bool kMulti, int kMaxThreads, int kMinBlocks, bool kRadial = false>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(const __grid_constant__ TransportArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -362,14 +364,12 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     const unsigned refill_min = (unsigned)a.refill;
     const unsigned fresnel_min = (unsigned)max(a.fresnel_batch, 1);
 
-    __shared__ RngKey s_key;
-    if (threadIdx.x < 20) s_key.rk[threadIdx.x] = a.round_keys[threadIdx.x];
-    if (threadIdx.x == 0) s_key.run = *a.run_tag;
     __syncthreads();
     Walker w;
     w.ring = s_uring + threadIdx.x;
     w.stride = blockDim.x;
-    w.key = &s_key;
+    w.key.rk = a.round_keys;
+    w.key.run = *a.run_tag;
     int prim = 0, geom = 0;
 
     for (;;) {
@@ -482,7 +482,12 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                 if (lane == __ffs(peers) - 1 && prim < a.n_prim) atomicAdd(&a.per_primary[prim], __popc(peers));
                 const int xdim = kMulti ? s_geom[geom].xdim : a.g0.xdim;
                 const int ydim = kMulti ? s_geom[geom].ydim : a.g0.ydim;
-                if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {
+                if (kRadial) {
+                    const float rx = w.px - w.ex, ry = w.py - w.ey;
+                    const int b = min((int)(sqrtf(rx * rx + ry * ry) * a.radial_inv_width), a.radial_bins);
+                    if (prim < a.n_prim && b >= 0)
+                        atomicAdd(&a.radial[(long long)prim * (a.radial_bins + 1) + b], 1u);
+                } else if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {
                     atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);
                     const int wx = w.ii - a.win_x0, wy = w.jj - a.win_y0;
                     if (geom == 0 && win > 0 && (unsigned)wx < (unsigned)win && (unsigned)wy < (unsigned)win) {
@@ -636,18 +641,19 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
 
 // Register budgets: blocks of up to 256 threads are compiled for 2, 3 or 4
 // resident CTAs per SM (128, 85, 64 registers); larger blocks for one.
-#define FD2_TRANSPORT_VARIANTS(X)        \
-    X(false, 512, 1) X(false, 256, 2)    \
-    X(false, 256, 3) X(false, 256, 4)    \
-    X(true, 512, 1) X(true, 256, 2) X(true, 256, 3)
+#define FD2_TRANSPORT_VARIANTS(X)                          \
+    X(false, 512, 1, false) X(false, 256, 2, false)        \
+    X(false, 256, 3, false) X(false, 256, 4, false)        \
+    X(true, 512, 1, false) X(true, 256, 2, false)          \
+    X(true, 256, 3, false) X(true, 256, 2, true)
 
 cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
 {
     const int bytes = (int)transport_smem_bytes(cfg, n_geom);
     cudaError_t e = cudaSuccess;
-#define FD2_SET_ATTR(M, T, B)                                                                                   \
+#define FD2_SET_ATTR(M, T, B, R)                                                                                \
     if (e == cudaSuccess)                                                                                       \
-        e = cudaFuncSetAttribute(transport_kernel<M, T, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(transport_kernel<M, T, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     FD2_TRANSPORT_VARIANTS(FD2_SET_ATTR)
 #undef FD2_SET_ATTR
     return e;
@@ -664,7 +670,11 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
     const unsigned grid = (unsigned)(sm_count * cfg.ctas_per_sm);
     const bool multi = a.n_geom > 1;
     const int per_sm = cfg.block > 256 ? 1 : std::min(std::max(cfg.ctas_per_sm, 2), multi ? 3 : 4);
-    if (!multi) {
+    if (a.radial) {
+        // label mode: one variant, 256 threads, two CTAs per SM
+        if (cfg.block > 256) return cudaErrorInvalidConfiguration;
+        transport_kernel<true, 256, 2, true><<<(unsigned)(sm_count * 2), cfg.block, smem, s>>>(a);
+    } else if (!multi) {
         if (per_sm == 1) transport_kernel<false, 512, 1><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 2) transport_kernel<false, 256, 2><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 3) transport_kernel<false, 256, 3><<<grid, cfg.block, smem, s>>>(a);

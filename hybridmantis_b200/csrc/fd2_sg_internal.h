@@ -1,0 +1,80 @@
+// fd2_sg_internal.h -- state of the surrogate (fd2_surrogate.h) shared by
+// its training code (fd2_surrogate.cu) and the event pipeline (fd2_sg_run.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "fd2_surrogate.h"
+
+namespace fd2 {
+namespace sg {
+
+constexpr int kFeatures = FD2_SG_FEATURES;
+constexpr int kOutputs = FD2_SG_OUTPUTS;
+constexpr int kComponents = FD2_SG_COMPONENTS;
+constexpr int kInPad = 32;   // input width seen by the first GEMM (K multiple of 32)
+constexpr int kOutPad = 64;  // output width of the last GEMM
+constexpr int kMaxSplits = 16;
+constexpr float kMuScale = 50.0f;  // um per unit of the mean outputs
+constexpr float kSdScale = 10.0f;  // um
+constexpr float kLogSdMin = -6.0f, kLogSdMax = 4.0f;
+
+// parameter blocks of the FP32 master vector
+enum { kW1 = 0, kB1, kW2, kB2, kW3, kB3, kW4, kB4, kNumBlocks };
+
+// x = 2 (f - lo) inv - 1 per feature
+struct NormParams {
+    float lo[kFeatures];
+    float inv[kFeatures];
+};
+
+}  // namespace sg
+}  // namespace fd2
+
+struct fd2_sg {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int hidden = 256, bins = 64, batch = 8192;
+    double radial_max = 200.0;
+    float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f, lambda = 1.0f;
+    uint64_t seed = 0;
+    fd2_sg_hull hull{};
+    fd2::sg::NormParams norm{};
+
+    // parameters (FP32 masters, gradients, Adam moments, BF16 copies)
+    int64_t off[fd2::sg::kNumBlocks] = {};
+    int64_t n_params = 0;
+    float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    __nv_bfloat16 *pb = nullptr;
+    uint8_t *d_live = nullptr;
+    unsigned long long *d_step = nullptr;
+    double *d_acc = nullptr;
+    float *ws = nullptr;  // split-K partials
+
+    // activations for up to cap_rows rows
+    int cap_rows = 0;
+    __nv_bfloat16 *x0 = nullptr, *h1 = nullptr, *h2 = nullptr, *h3 = nullptr;
+    __nv_bfloat16 *d1 = nullptr, *d2 = nullptr, *d3 = nullptr, *dout = nullptr;
+    float *out = nullptr, *target = nullptr, *ylab = nullptr, *has_rad = nullptr;
+    cudaGraphExec_t graph = nullptr;
+
+    // training data
+    int64_t n_points = 0, n_train = 0, n_val = 0;
+    float *d_feat = nullptr;
+    int32_t *d_photons = nullptr, *d_detected = nullptr;
+    uint32_t *d_radial = nullptr;
+
+    // event-pipeline buffers (fd2_sg_run)
+    struct RunBuffers *run = nullptr;
+};
+
+fd2_status sg_fail(fd2_sg *s, fd2_status st, const std::string &msg);
+fd2_status sg_cuda(fd2_sg *s, cudaError_t e, const char *what);
+cudaError_t sg_forward(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *x0, int rows, const int *m_limit,
+                       __nv_bfloat16 *h1, __nv_bfloat16 *h2, __nv_bfloat16 *h3, float *out);
+void sg_free_run_buffers(fd2_sg *s);

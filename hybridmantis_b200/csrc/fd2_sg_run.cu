@@ -1,0 +1,575 @@
+// fd2_sg_run.cu -- the surrogate in the event pipeline (fd2_sg_run).
+//
+// One run over a context's resident events:
+//   1. photon counts per event (the context's count pass: Poisson, Gaussian
+//      or given, exactly as fd2_run samples them);
+//   2. routing: every event whose features lie in the training hull becomes
+//      a surrogate row (its network input is written, its photon count is
+//      taken out of the Monte Carlo queue); a hash of the event index picks
+//      the audit fraction among them;
+//   3. the Monte Carlo transports what is left (events outside the hull);
+//   4. the network runs on all surrogate rows (GEMM grid sized for every
+//      event, rows beyond the device-side row count skipped);
+//   5. sampling, one warp per row: detected count ~ Binomial(N, p) split over
+//      the 32 lanes (geometric skipping), then each detected photon's radius
+//      from the truncated mixture, a uniform azimuth, and the PRF pixel;
+//      per-history counts and counters as the Monte Carlo tallies them;
+//   6. PHS and the run counter (the context's last pipeline segment);
+//   7. audit: the audited rows' depositions are transported by the Monte
+//      Carlo in label mode and compared with their predictions.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fd2.h"
+#include "fd2_ctx.h"
+#include "fd2_internal.h"
+#include "fd2_sg_gemm.cuh"
+#include "fd2_sg_internal.h"
+#include "fd2_surrogate.h"
+
+using namespace fd2::sg;
+
+struct RunBuffers {
+    int64_t cap = 0;
+    int *d_count = nullptr;          // [0] surrogate rows, [1] audit rows, [2] Monte Carlo events
+    int32_t *sg_event = nullptr;     // event of each surrogate row
+    int32_t *sg_n = nullptr;         // photons of each surrogate row
+    int32_t *audit_row = nullptr;    // surrogate row of each audit entry
+    __nv_bfloat16 *x0 = nullptr, *ha = nullptr, *hb = nullptr;
+    float *out = nullptr;
+    unsigned long long *d_stat = nullptr;  // [0] surrogate photons, [1] detected
+    // audit gather (compact copies of the audited rows)
+    float4 *a_pos = nullptr;
+    int32_t *a_n = nullptr, *a_geom = nullptr;
+    float *a_out = nullptr;
+    int64_t a_cap = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+void sg_free_run_buffers(fd2_sg *s)
+{
+    RunBuffers *r = s->run;
+    if (!r) return;
+    for (void *p : {(void *)r->d_count, (void *)r->sg_event, (void *)r->sg_n, (void *)r->audit_row, (void *)r->x0,
+                    (void *)r->ha, (void *)r->hb, (void *)r->out, (void *)r->d_stat, (void *)r->a_pos,
+                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_out})
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : r->ev)
+        if (e) cudaEventDestroy(e);
+    delete r;
+    s->run = nullptr;
+}
+
+namespace {
+
+__device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// uniform in (0, 1): (k + 0.5) 2^-24
+__device__ __forceinline__ float unit(uint32_t r) { return ((float)(r >> 8) + 0.5f) * 5.9604644775390625e-8f; }
+
+constexpr uint32_t kDomainAudit = 0x41554449u;   // audit selection
+constexpr uint32_t kDomainBinom = 0x42494e4fu;   // detected counts
+constexpr uint32_t kDomainPlace = 0x504c4143u;   // photon positions
+
+struct RouteArgs {
+    int64_t n;
+    const float4 *ev_pos;
+    const double *ev_e;
+    const uint16_t *ev_geom;
+    const fd2::DevGeom *geoms;
+    int32_t *ev_n;
+    uint32_t *ev_nchunks;
+    NormParams norm;
+    fd2_sg_hull hull;
+    float audit_frac;
+    uint32_t k0, k1;
+    int64_t event_base;
+    int *count;
+    int32_t *sg_event, *sg_n, *audit_row;
+    __nv_bfloat16 *x0;
+};
+
+__global__ void route_kernel(const RouteArgs a)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t N = a.ev_n[e];
+        if (N <= 0) continue;
+        const fd2::DevGeom &g = a.geoms[a.ev_geom ? a.ev_geom[e] : 0];
+        const float4 p = a.ev_pos[e];
+        float f[kFeatures];
+        f[0] = g.half - p.z;                 // depth below the entrance surface
+        f[1] = (float)(a.ev_e[e] * 1e-3);    // keV
+        f[2] = 0.5f;                          // in-column offset: no effect in the walk
+        f[3] = g.H;
+        f[4] = g.R;
+        f[5] = g.beta;
+        f[6] = 1.0f - g.top_absfrac;
+        f[7] = g.mu > 0.0f ? log10f(g.mu) : -INFINITY;
+        bool in = true;
+#pragma unroll
+        for (int i = 0; i < kFeatures; ++i) in = in && f[i] >= a.hull.lo[i] && f[i] <= a.hull.hi[i];
+        if (!in) {
+            atomicAdd(&a.count[2], 1);
+            continue;
+        }
+        const int row = atomicAdd(&a.count[0], 1);
+        a.sg_event[row] = (int32_t)e;
+        a.sg_n[row] = N;
+        __nv_bfloat16 *x = a.x0 + (int64_t)row * kInPad;
+#pragma unroll
+        for (int i = 0; i < kFeatures; ++i)
+            x[i] = __float2bfloat16(2.0f * (f[i] - a.norm.lo[i]) * a.norm.inv[i] - 1.0f);
+#pragma unroll
+        for (int i = kFeatures; i < kInPad; ++i) x[i] = __float2bfloat16(0.0f);
+        a.ev_n[e] = 0;          // out of the Monte Carlo queue
+        a.ev_nchunks[e] = 0;
+        const uint64_t ge = (uint64_t)(a.event_base + e);
+        const uint4 h = philox10(make_uint4((uint32_t)ge, (uint32_t)(ge >> 32), kDomainAudit, 0), a.k0, a.k1);
+        if (unit(h.x) < a.audit_frac) a.audit_row[atomicAdd(&a.count[1], 1)] = row;
+    }
+}
+
+struct SampleArgs {
+    const int *count;
+    int32_t *ev_n;
+    const int32_t *sg_event, *sg_n;
+    const float *out;
+    const float4 *ev_pos;
+    const uint16_t *ev_geom;
+    const fd2::DevGeom *geoms;
+    unsigned long long *prf;
+    int32_t *per_primary;
+    int32_t n_prim;
+    unsigned long long *counters;
+    unsigned long long *stat;
+    uint32_t k0, k1;
+    int64_t event_base;
+    const uint32_t *run_tag;
+};
+
+// Detected photons of one row and their PRF pixels; one warp per row.
+__global__ void sample_kernel(const SampleArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const int rows = *a.count;
+    const uint32_t run = *a.run_tag;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+        const int64_t e = a.sg_event[r];
+        const int32_t N = a.sg_n[r];
+        const float *o = a.out + (int64_t)r * kOutPad;
+        const uint16_t gi = a.ev_geom ? a.ev_geom[e] : 0;
+        const fd2::DevGeom &g = a.geoms[gi];
+        const float4 pos = a.ev_pos[e];
+        const uint64_t ge = (uint64_t)(a.event_base + e);
+        // ---- detected count: lane l takes photons [lo, hi) of the N
+        const float z = o[0];
+        const float p = 1.0f / (1.0f + expf(-z));
+        const int32_t lo = (int32_t)(((int64_t)N * lane) >> 5), hi = (int32_t)(((int64_t)N * (lane + 1)) >> 5);
+        const int32_t m = hi - lo;
+        int32_t k = 0;
+        if (m > 0 && p > 0.0f) {
+            if (p >= 1.0f) {
+                k = m;
+            } else {
+                // count the rarer outcome by geometric skips: expected m min(p, 1 - p) + 1 draws
+                const bool flip = p > 0.5f;
+                const float q = flip ? 1.0f - p : p;
+                const float inv_log = 1.0f / log1pf(-q);
+                int32_t hits = 0, at = -1;
+                uint32_t ctr = 0;
+                for (;;) {
+                    const uint4 h = philox10(make_uint4(ctr++, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainBinom,
+                                                        run * 32u + (uint32_t)lane),
+                                             a.k0, a.k1);
+                    const uint32_t w4[4] = {h.x, h.y, h.z, h.w};
+                    bool done = false;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float skip = floorf(logf(unit(w4[j])) * inv_log);
+                        const float next = (float)at + skip + 1.0f;
+                        if (next >= (float)m) {
+                            done = true;
+                            break;
+                        }
+                        at = (int32_t)next;
+                        ++hits;
+                    }
+                    if (done) break;
+                }
+                k = flip ? m - hits : hits;
+            }
+        }
+        // warp total and this lane's first detected index
+        int32_t before = k;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int32_t v = __shfl_up_sync(0xffffffffu, before, d);
+            if (lane >= d) before += v;
+        }
+        const int32_t total = __shfl_sync(0xffffffffu, before, 31);
+        // ---- positions of the detected photons from the truncated mixture
+        float w[kComponents], mu[kComponents], sd[kComponents], c0[kComponents], S[kComponents];
+        {
+            float amax = o[1];
+            for (int c = 1; c < kComponents; ++c) amax = fmaxf(amax, o[1 + c]);
+            float tot = 0.0f;
+            for (int c = 0; c < kComponents; ++c) {
+                mu[c] = kMuScale * o[1 + kComponents + c];
+                sd[c] = kSdScale * expf(fminf(fmaxf(o[1 + 2 * kComponents + c], kLogSdMin), kLogSdMax));
+                c0[c] = normcdff(-mu[c] / sd[c]);
+                S[c] = 1.0f - c0[c];
+                w[c] = expf(o[1 + c] - amax) * S[c];
+                tot += w[c];
+            }
+            float acc = 0.0f;
+            for (int c = 0; c < kComponents; ++c) {
+                acc += w[c] / tot;
+                w[c] = acc;  // cumulative
+            }
+            w[kComponents - 1] = 2.0f;
+        }
+        int32_t in_prf = 0;
+        for (int32_t i = lane; i < total; i += 32) {
+            const uint4 h = philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainPlace, run),
+                                     a.k0, a.k1);
+            const float u1 = unit(h.x);
+            int c = 0;
+            while (c < kComponents - 1 && u1 >= w[c]) ++c;
+            const float qv = fminf(fmaxf(c0[c] + unit(h.y) * S[c], 1e-7f), 1.0f - 6e-8f);
+            const float rad = fmaxf(mu[c] + sd[c] * normcdfinvf(qv), 0.0f);
+            float sn, cs;
+            sincospif(2.0f * unit(h.z), &sn, &cs);
+            const float x = pos.x + rad * cs, y = pos.y + rad * sn;
+            if (x <= g.ub_x && y <= g.ub_y && x >= g.lb_x && y >= g.lb_y) {
+                const int ii = (int)floorf(__fdiv_rn(x - g.lb_x, g.pixel));
+                const int jj = (int)floorf(__fdiv_rn(y - g.lb_y, g.pixel));
+                if (ii >= 0 && jj >= 0 && ii < g.xdim && jj < g.ydim) {
+                    atomicAdd(&a.prf[g.prf_offset + (long long)ii * g.ydim + jj], 1ull);
+                    ++in_prf;
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) in_prf += __shfl_down_sync(0xffffffffu, in_prf, d);
+        if (lane == 0) {
+            a.ev_n[e] = N;  // the run's photon count, as fd2_get_photon_counts reports it
+            const int prim = __float_as_int(pos.w);
+            if (total > 0 && prim >= 0 && prim < a.n_prim) atomicAdd(&a.per_primary[prim], total);
+            unsigned long long *cn = a.counters + (long long)gi * fd2::kCounterStride;
+            if (total > 0) atomicAdd(&cn[fd2::kDetect], (unsigned long long)total);
+            if (in_prf > 0) atomicAdd(&cn[fd2::kNumFates], (unsigned long long)in_prf);
+            atomicAdd(&a.stat[0], (unsigned long long)N);
+            atomicAdd(&a.stat[1], (unsigned long long)total);
+        }
+    }
+}
+
+// Compact copies of the audited rows.
+__global__ void audit_gather_kernel(const int *count, const int32_t *audit_row, const int32_t *sg_event,
+                                    const int32_t *sg_n, const float *out, const float4 *ev_pos,
+                                    const uint16_t *ev_geom, float4 *a_pos, int32_t *a_n, int32_t *a_geom,
+                                    float *a_out)
+{
+    const int n = count[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int r = audit_row[i];
+        const int32_t e = sg_event[r];
+        a_pos[i] = ev_pos[e];
+        a_n[i] = sg_n[r];
+        a_geom[i] = ev_geom ? ev_geom[e] : 0;
+        for (int k = 0; k < kOutputs; ++k) a_out[(int64_t)i * kOutputs + k] = out[(int64_t)r * kOutPad + k];
+    }
+}
+
+template <class T>
+cudaError_t alloc(T **p, size_t n)
+{
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(n, 1));
+}
+
+fd2_status ensure_run_buffers(fd2_sg *s, int64_t n)
+{
+    if (!s->run) {
+        s->run = new RunBuffers();
+        for (auto &e : s->run->ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return sg_fail(s, FD2_ERR_CUDA, "event create");
+        if (alloc(&s->run->d_count, 3) != cudaSuccess || alloc(&s->run->d_stat, 2) != cudaSuccess)
+            return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "run buffers");
+    }
+    RunBuffers *r = s->run;
+    if (n <= r->cap) return FD2_OK;
+    const size_t N = (size_t)n, H = (size_t)s->hidden;
+    if (alloc(&r->sg_event, N) || alloc(&r->sg_n, N) || alloc(&r->audit_row, N) || alloc(&r->x0, N * kInPad) ||
+        alloc(&r->ha, N * H) || alloc(&r->hb, N * H) || alloc(&r->out, N * kOutPad))
+        return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "run buffers for " + std::to_string(n) + " events");
+    r->cap = n;
+    return FD2_OK;
+}
+
+double phi_cdf(double x) { return 0.5 * std::erfc(-x / std::sqrt(2.0)); }
+
+// Bin probabilities of one row's truncated mixture (bins + 1 categories).
+void bin_probs(const float *o, int bins, double width, double *q)
+{
+    double w[kComponents], mu[kComponents], sd[kComponents];
+    double amax = o[1];
+    for (int k = 1; k < kComponents; ++k) amax = std::max(amax, (double)o[1 + k]);
+    double ws = 0.0;
+    for (int k = 0; k < kComponents; ++k) {
+        w[k] = std::exp(o[1 + k] - amax);
+        ws += w[k];
+        mu[k] = kMuScale * o[1 + kComponents + k];
+        sd[k] = kSdScale * std::exp(std::min(std::max((double)o[1 + 2 * kComponents + k], (double)kLogSdMin),
+                                             (double)kLogSdMax));
+    }
+    double Z = 0.0;
+    for (int k = 0; k < kComponents; ++k) Z += w[k] / ws * phi_cdf(mu[k] / sd[k]);
+    for (int j = 0; j <= bins; ++j) {
+        double A = 0.0;
+        for (int k = 0; k < kComponents; ++k) {
+            const double alo = (j * width - mu[k]) / sd[k];
+            const double ahi = j < bins ? ((j + 1) * width - mu[k]) / sd[k] : INFINITY;
+            // lower-tail differences left of the mean, upper-tail ones right of it
+            const double P = alo >= 0.0 ? phi_cdf(-alo) - (j < bins ? phi_cdf(-ahi) : 0.0)
+                                        : (j < bins ? phi_cdf(ahi) : 1.0) - phi_cdf(alo);
+            A += w[k] / ws * std::max(P, 0.0);
+        }
+        q[j] = Z > 0 ? A / Z : 0.0;
+    }
+}
+
+}  // namespace
+
+extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, fd2_sg_stats *stats)
+{
+    if (!s || !c || !(audit_fraction >= 0.0 && audit_fraction <= 1.0)) return FD2_ERR_INVALID_ARGUMENT;
+    if (c->device != s->device) return sg_fail(s, FD2_ERR_INVALID_ARGUMENT, "surrogate and context on different GPUs");
+    if (c->d_radial) return sg_fail(s, FD2_ERR_STATE, "the context is in label mode");
+    fd2_status st = fd2_wait(c);
+    if (st != FD2_OK) return sg_fail(s, st, std::string("context: ") + fd2_last_error(c));
+    if (c->n_events <= 0) return sg_fail(s, FD2_ERR_STATE, "no events submitted");
+    if (cudaSetDevice(c->device) != cudaSuccess) return sg_fail(s, FD2_ERR_CUDA, "set device");
+    if ((st = fd2::api::ensure_chunks(c)) != FD2_OK) return sg_fail(s, st, "context chunks");
+    const int64_t n = c->n_events;
+    // the network's GEMM grid has one row of CTAs per 64 events
+    if (n > (int64_t)65535 * kBM) return sg_fail(s, FD2_ERR_INVALID_ARGUMENT, "more than 4,194,240 events per run");
+    if ((st = ensure_run_buffers(s, n)) != FD2_OK) return st;
+    RunBuffers *R = s->run;
+    cudaStream_t q = c->stream;
+    const auto t_start = std::chrono::steady_clock::now();
+    const uint32_t k0 = (uint32_t)c->opt.seed ^ 0x53475255u, k1 = (uint32_t)(c->opt.seed >> 32) ^ 0x4e5f4b31u;
+    cudaError_t e = cudaEventRecord(R->ev[0], q);
+    if (e == cudaSuccess) e = cudaMemsetAsync(R->d_count, 0, 3 * sizeof(int), q);
+    if (e == cudaSuccess) e = cudaMemsetAsync(R->d_stat, 0, 2 * sizeof(unsigned long long), q);
+    // 1-2: counts, routing
+    if (e == cudaSuccess) e = fd2::api::count_pass(c, true);
+    if (e == cudaSuccess) {
+        RouteArgs a;
+        a.n = n;
+        a.ev_pos = c->d_ev_pos;
+        a.ev_e = c->d_ev_e;
+        a.ev_geom = c->has_geom ? c->d_ev_geom : nullptr;
+        a.geoms = c->d_geoms;
+        a.ev_n = c->d_ev_n;
+        a.ev_nchunks = c->d_ev_nchunks;
+        a.norm = s->norm;
+        // the hull, widened by a few float ulps: geometry features computed
+        // on the device (log10f, 1 - top_absfrac) may differ from the host's
+        // by rounding
+        a.hull = s->hull;
+        for (int i = 0; i < kFeatures; ++i) {
+            const float tol = 1e-5f * std::max(1.0f, std::max(std::fabs(a.hull.lo[i]), std::fabs(a.hull.hi[i])));
+            a.hull.lo[i] -= tol;
+            a.hull.hi[i] += tol;
+        }
+        a.audit_frac = (float)audit_fraction;
+        a.k0 = k0;
+        a.k1 = k1;
+        a.event_base = c->opt.event_base;
+        a.count = R->d_count;
+        a.sg_event = R->sg_event;
+        a.sg_n = R->sg_n;
+        a.audit_row = R->audit_row;
+        a.x0 = R->x0;
+        route_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 8192), 256, 0, q>>>(a);
+        e = cudaGetLastError();
+    }
+    // 3: Monte Carlo for the rest
+    if (e == cudaSuccess)
+        e = fd2::launch_scan(q, n, c->d_ev_nchunks, c->d_chunk_off, c->d_block_sums, c->d_scalars + 0);
+    if (e == cudaSuccess)
+        e = fd2::launch_fill_chunks(q, n, c->cfg.chunk, c->d_ev_n, c->d_chunk_off, c->d_chunks, c->chunk_cap,
+                                    c->d_flags);
+    if (e == cudaSuccess) e = cudaEventRecord(R->ev[1], q);
+    if (e == cudaSuccess) e = fd2::launch_transport(q, c->cfg, c->sm_count, fd2::api::transport_args(c));
+    if (e == cudaSuccess) e = cudaEventRecord(R->ev[2], q);
+    // 4-5: network and sampling
+    if (e == cudaSuccess) e = sg_forward(s, q, R->x0, (int)n, R->d_count, R->ha, R->hb, R->ha, R->out);
+    if (e == cudaSuccess) {
+        SampleArgs a;
+        a.count = R->d_count;
+        a.ev_n = c->d_ev_n;
+        a.sg_event = R->sg_event;
+        a.sg_n = R->sg_n;
+        a.out = R->out;
+        a.ev_pos = c->d_ev_pos;
+        a.ev_geom = c->has_geom ? c->d_ev_geom : nullptr;
+        a.geoms = c->d_geoms;
+        a.prf = c->d_prf;
+        a.per_primary = c->d_per_primary;
+        a.n_prim = c->n_prim;
+        a.counters = c->d_counters;
+        a.stat = R->d_stat;
+        a.k0 = k0;
+        a.k1 = k1;
+        a.event_base = c->opt.event_base;
+        a.run_tag = reinterpret_cast<const uint32_t *>(c->d_flags + 1);
+        sample_kernel<<<(unsigned)(c->sm_count * 8), 256, 0, q>>>(a);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(R->ev[3], q);
+    // 6: PHS and the run counter
+    if (e == cudaSuccess) e = fd2::api::enqueue_segment(c, 2);
+    int counts[3] = {0, 0, 0};
+    unsigned long long stat[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counts, R->d_count, sizeof counts, cudaMemcpyDeviceToHost, q);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stat, R->d_stat, sizeof stat, cudaMemcpyDeviceToHost, q);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+    if (e != cudaSuccess) return sg_cuda(s, e, "surrogate run");
+    c->counts_ready = true;
+    c->ran_once = true;
+    c->graph_valid = false;  // the counts were rewritten outside the graph
+    if ((st = fd2::api::check_status(c)) != FD2_OK) return sg_fail(s, st, std::string("context: ") + fd2_last_error(c));
+    float mc_ms = 0, sg_ms = 0;
+    cudaEventElapsedTime(&mc_ms, R->ev[1], R->ev[2]);
+    cudaEventElapsedTime(&sg_ms, R->ev[2], R->ev[3]);
+    const double run_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+
+    // 7: audit
+    fd2_sg_stats out;
+    std::memset(&out, 0, sizeof out);
+    out.events = n;
+    out.surrogate_events = counts[0];
+    out.audit_events = counts[1];
+    out.surrogate_photons = (int64_t)stat[0];
+    out.surrogate_detected = (int64_t)stat[1];
+    out.sg_ms = sg_ms;
+    out.mc_ms = mc_ms;
+    const auto t_audit = std::chrono::steady_clock::now();
+    const int na = counts[1];
+    if (na > 0) {
+        RunBuffers *B = R;
+        if (na > B->a_cap) {
+            if (alloc(&B->a_pos, (size_t)na) || alloc(&B->a_n, (size_t)na) || alloc(&B->a_geom, (size_t)na) ||
+                alloc(&B->a_out, (size_t)na * kOutputs))
+                return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "audit buffers");
+            B->a_cap = na;
+        }
+        audit_gather_kernel<<<(unsigned)std::min((na + 255) / 256, 4096), 256, 0, q>>>(
+            R->d_count, R->audit_row, R->sg_event, R->sg_n, R->out, c->d_ev_pos, c->has_geom ? c->d_ev_geom : nullptr,
+            B->a_pos, B->a_n, B->a_geom, B->a_out);
+        std::vector<float4> pos((size_t)na);
+        std::vector<int32_t> nph((size_t)na), geo((size_t)na);
+        std::vector<float> ao((size_t)na * kOutputs);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(pos.data(), B->a_pos, sizeof(float4) * na, cudaMemcpyDeviceToHost, q);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(nph.data(), B->a_n, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(geo.data(), B->a_geom, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ao.data(), B->a_out, sizeof(float) * na * kOutputs, cudaMemcpyDeviceToHost, q);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+        if (e != cudaSuccess) return sg_cuda(s, e, "audit gather");
+        // the audited depositions through the Monte Carlo, label mode
+        fd2_params ap = c->params;
+        ap.num_hist = na;
+        fd2_options ao_opt = c->opt;
+        ao_opt.count_mode = FD2_COUNT_GIVEN;
+        ao_opt.seed = c->opt.seed ^ 0xA0D17A0D17ull;
+        ao_opt.radial_bins = s->bins;
+        ao_opt.radial_max_um = s->radial_max;
+        ao_opt.event_base = 0;
+        ao_opt.tune_cache = nullptr;
+        ao_opt.wait_timeout_s = 0.0;
+        fd2_ctx *ac = nullptr;
+        st = fd2_create(&ap, &ao_opt, &ac);
+        if (st == FD2_OK && c->geoms.size() > 1) st = fd2_set_geometries(ac, c->geoms.data(), (int32_t)c->geoms.size());
+        std::vector<float> xs((size_t)na), ys((size_t)na), zs((size_t)na);
+        std::vector<int32_t> hist((size_t)na);
+        std::vector<uint16_t> gg((size_t)na);
+        for (int i = 0; i < na; ++i) {
+            xs[(size_t)i] = pos[(size_t)i].x;
+            ys[(size_t)i] = pos[(size_t)i].y;
+            zs[(size_t)i] = pos[(size_t)i].z;
+            hist[(size_t)i] = i + 1;
+            gg[(size_t)i] = (uint16_t)geo[(size_t)i];
+        }
+        if (st == FD2_OK)
+            st = fd2_submit_events_um(ac, xs.data(), ys.data(), zs.data(), nullptr, hist.data(), nph.data(),
+                                      c->geoms.size() > 1 ? gg.data() : nullptr, na);
+        if (st == FD2_OK) st = fd2_run(ac);
+        if (st == FD2_OK) st = fd2_wait(ac);
+        std::vector<int32_t> det((size_t)na);
+        const int nb = s->bins + 1;
+        std::vector<uint32_t> rad((size_t)na * nb);
+        if (st == FD2_OK) st = fd2_get_detected_per_primary(ac, det.data(), na);
+        if (st == FD2_OK) st = fd2_get_radial(ac, rad.data(), (int64_t)rad.size());
+        const std::string aerr = ac ? fd2_last_error(ac) : "";
+        fd2_destroy(ac);
+        if (st != FD2_OK) return sg_fail(s, st, "audit Monte Carlo: " + aerr);
+        double mc = 0, expct = 0, var = 0, ph = 0;
+        std::vector<double> hmc((size_t)nb, 0.0), hsg((size_t)nb, 0.0), qv((size_t)nb);
+        const double width = s->radial_max / s->bins;
+        for (int i = 0; i < na; ++i) {
+            const float *o = &ao[(size_t)i * kOutputs];
+            const double p = 1.0 / (1.0 + std::exp(-(double)o[0]));
+            const double N = nph[(size_t)i];
+            mc += det[(size_t)i];
+            expct += N * p;
+            var += N * p * (1.0 - p);
+            ph += N;
+            bin_probs(o, s->bins, width, qv.data());
+            for (int j = 0; j < nb; ++j) {
+                hmc[(size_t)j] += rad[(size_t)i * nb + j];
+                hsg[(size_t)j] += N * p * qv[(size_t)j];
+            }
+        }
+        double smc = 0, ssg = 0, l1 = 0;
+        for (int j = 0; j < nb; ++j) {
+            smc += hmc[(size_t)j];
+            ssg += hsg[(size_t)j];
+        }
+        for (int j = 0; j < nb; ++j)
+            l1 += std::fabs((smc > 0 ? hmc[(size_t)j] / smc : 0) - (ssg > 0 ? hsg[(size_t)j] / ssg : 0));
+        out.audit_mc_detected = mc;
+        out.audit_sg_expected = expct;
+        out.audit_photons = ph;
+        out.audit_z = var > 0 ? (mc - expct) / std::sqrt(var) : 0.0;
+        out.audit_radial_l1 = l1;
+    }
+    out.audit_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_audit).count();
+    out.total_ms = (float)(run_ms + out.audit_ms);
+    out.mc_events = counts[2];
+    if (stats) *stats = out;
+    return FD2_OK;
+}

@@ -161,7 +161,8 @@ class OpticalTransport:
     def __init__(self, params: Params, *, device: int = 0, count_mode: int = COUNT_POISSON, seed: int | None = None,
                  block_size: int = 0, ctas_per_sm: int = 0, chunk: int = 0, refill: int = 0, prf_window: int = -1,
                  use_graph: bool = True, wait_timeout_s: float = 0.0, max_photons_per_event: int = 900000,
-                 tune_cache: str | None = None, event_base: int = 0, fresnel_batch: int = 0):
+                 tune_cache: str | None = None, event_base: int = 0, fresnel_batch: int = 0,
+                 radial_bins: int = 0, radial_max_um: float = 200.0):
         lib = load()
         self._lib = lib
         opt = Options()
@@ -177,6 +178,9 @@ class OpticalTransport:
         opt.max_photons_per_event = max_photons_per_event
         opt.event_base = event_base
         opt.fresnel_batch = fresnel_batch
+        opt.radial_bins = radial_bins
+        opt.radial_max_um = radial_max_um
+        self.radial_bins = radial_bins
         self._tune_cache = tune_cache.encode() if tune_cache else None
         opt.tune_cache = self._tune_cache
         self.params = params
@@ -273,6 +277,14 @@ class OpticalTransport:
         out = np.zeros(max(self.params.num_hist, 1), np.int32)
         self._check(self._lib.fd2_get_detected_per_primary(self._h, ptr(out), out.size), "get_detected_per_primary")
         return out[:self.params.num_hist]
+
+    def radial(self) -> np.ndarray:
+        """Label mode: [num_hist, radial_bins + 1] detected photons by distance
+        from their event (last column: beyond radial_max_um)."""
+        nb = self.radial_bins + 1
+        out = np.zeros(max(self.params.num_hist, 1) * nb, np.uint32)
+        self._check(self._lib.fd2_get_radial(self._h, ptr(out), out.size), "get_radial")
+        return out.reshape(-1, nb)[:self.params.num_hist]
 
     def photon_counts(self, n_events: int) -> np.ndarray:
         out = np.zeros(max(n_events, 1), np.int32)

@@ -1,0 +1,238 @@
+"""Learned surrogate of the optical transport (include/fd2_surrogate.h).
+
+``label_points`` produces training data with this library's own Monte Carlo
+in label mode: every point is one deposition transported with a fixed number
+of photons, and its label is the detected count and the radial histogram of
+the detected photons around it.  ``Surrogate`` wraps the C ABI: BF16
+tensor-core training on the GPU, prediction, and the surrogate-in-the-loop
+event pipeline (``run``).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import Geometry, SgConfig, SgHull, SgStats, check, load, ptr
+from .fastdetect2 import COUNT_GIVEN, OpticalTransport, default_params
+
+FEATURES = ["depth_um", "energy_kev", "offset", "thickness_um", "radius_um", "beta", "top_reflectivity",
+            "log10_mu"]
+N_FEATURES = 8
+N_OUTPUTS = 25
+N_COMPONENTS = 8
+MU_SCALE, SD_SCALE = 50.0, 10.0
+
+
+def geometry_features(g: Geometry) -> np.ndarray:
+    """Features 3..7 of a geometry."""
+    return np.array([g.det_height, g.radius, g.beta, 1.0 - g.top_absfrac, np.log10(max(g.bulk_abs, 1e-30))],
+                    np.float32)
+
+
+def features(depth_um, energy_kev, offset, g: Geometry) -> np.ndarray:
+    depth_um = np.asarray(depth_um, np.float32)
+    n = depth_um.size
+    f = np.empty((n, N_FEATURES), np.float32)
+    f[:, 0] = depth_um
+    f[:, 1] = energy_kev
+    f[:, 2] = offset
+    f[:, 3:] = geometry_features(g)
+    return f
+
+
+def sample_geometries(n: int, seed: int, base: Geometry | None = None) -> list:
+    """Detector geometries over the batched-workload ranges: thickness
+    U(100, 600) um, column radius U(2.5, 7.5) um, roughness U(0, 0.5), top
+    reflectivity U(0, 1), bulk absorption log-uniform on [1e-5, 1e-3] /um;
+    the other parameters from `base` (default: the benchmark detector)."""
+    rng = np.random.default_rng(seed)
+    if base is None:
+        base = _lib.Geometry()
+        load().fd2_params_to_geometry(ctypes.byref(default_params()), ctypes.byref(base))
+    out = []
+    for _ in range(n):
+        g = Geometry.from_buffer_copy(base)
+        g.det_height = rng.uniform(100.0, 600.0)
+        g.radius = rng.uniform(2.5, 7.5)
+        g.beta = rng.uniform(0.0, 0.5)
+        g.top_absfrac = 1.0 - rng.uniform(0.0, 1.0)
+        g.bulk_abs = float(np.exp(rng.uniform(np.log(1e-5), np.log(1e-3))))
+        out.append(g)
+    return out
+
+
+def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: int = 0, radial_bins: int = 64,
+                 radial_max_um: float = 200.0, energy_kev=(1.0, 80.0)):
+    """Monte Carlo labels: for each geometry, `points_per_geom` depositions at
+    the detector centre with depth U(0, H), energy U(energy_kev) and in-column
+    offset U(0, 1), each transported with `photons` photons.  Returns
+    (features [n, 8], photons [n], detected [n], radial [n, radial_bins + 1])."""
+    rng = np.random.default_rng(seed)
+    feats, phot, det, rad = [], [], [], []
+    for g0 in range(0, len(geoms), 256):
+        gs = list(geoms[g0:g0 + 256])
+        n = len(gs) * points_per_geom
+        p = default_params(num_hist=n)
+        with OpticalTransport(p, device=device, count_mode=COUNT_GIVEN, seed=seed + 7919 * g0,
+                              radial_bins=radial_bins, radial_max_um=radial_max_um) as t:
+            t.set_geometries(gs)
+            gi = np.repeat(np.arange(len(gs)), points_per_geom).astype(np.uint16)
+            H = np.array([g.det_height for g in gs])[gi]
+            depth = (H * rng.uniform(0.001, 0.999, n)).astype(np.float32).astype(np.float64)
+            cx = np.array([g.det_x / 2.0 for g in gs])[gi]
+            cy = np.array([g.det_y / 2.0 for g in gs])[gi]
+            z = H / 2.0 - depth
+            energy = rng.uniform(energy_kev[0], energy_kev[1], n)
+            offset = rng.uniform(0.0, 1.0, n)
+            nph = np.full(n, photons, np.int32)
+            t.submit_events_um(cx, cy, z, energy * 1000.0, np.arange(1, n + 1), nphot=nph, geom=gi)
+            t.run_sync()
+            d = t.detected_per_primary()
+            r = t.radial()
+        f = np.empty((n, N_FEATURES), np.float32)
+        f[:, 0] = depth
+        f[:, 1] = energy
+        f[:, 2] = offset
+        f[:, 3:] = np.stack([geometry_features(g) for g in gs])[gi]
+        feats.append(f)
+        phot.append(nph)
+        det.append(d.astype(np.int32))
+        rad.append(r.astype(np.uint32))
+    return np.concatenate(feats), np.concatenate(phot), np.concatenate(det), np.concatenate(rad)
+
+
+def mixture(out: np.ndarray):
+    """Decode network outputs [n, 25] into (p_detect [n], w [n, 8], mu [n, 8], sd [n, 8]) in um."""
+    out = np.asarray(out, np.float64)
+    p = 1.0 / (1.0 + np.exp(-out[:, 0]))
+    a = out[:, 1:1 + N_COMPONENTS]
+    w = np.exp(a - a.max(1, keepdims=True))
+    w /= w.sum(1, keepdims=True)
+    mu = MU_SCALE * out[:, 1 + N_COMPONENTS:1 + 2 * N_COMPONENTS]
+    sd = SD_SCALE * np.exp(np.clip(out[:, 1 + 2 * N_COMPONENTS:], -6.0, 4.0))
+    return p, w, mu, sd
+
+
+def radial_bin_probs(out: np.ndarray, bins: int = 64, radial_max_um: float = 200.0) -> np.ndarray:
+    """Bin probabilities [n, bins + 1] of the truncated mixture (last: overflow)."""
+    from scipy.special import ndtr
+    _, w, mu, sd = mixture(out)
+    edges = np.arange(bins + 1) * (radial_max_um / bins)
+    a = (edges[None, None, :] - mu[:, :, None]) / sd[:, :, None]
+    a = np.concatenate([a, np.full(a.shape[:2] + (1,), np.inf)], axis=2)
+    c, cc = ndtr(a), ndtr(-a)
+    S = ndtr(mu / sd)
+    lo = a[:, :, :-1]
+    P = np.maximum(np.where(lo >= 0, cc[:, :, :-1] - cc[:, :, 1:], c[:, :, 1:] - c[:, :, :-1]), 0.0)
+    A = (w[:, :, None] * P).sum(1)
+    Z = (w * S).sum(1, keepdims=True)
+    return A / Z
+
+
+class Surrogate:
+    """One surrogate network with its optimizer state on a GPU."""
+
+    def __init__(self, device: int = 0, hidden: int = 256, radial_bins: int = 64, radial_max_um: float = 200.0,
+                 batch: int = 8192, lr: float = 1e-3, radial_weight: float = 1.0, seed: int = 0x5347fd2):
+        lib = load()
+        self._lib = lib
+        c = SgConfig()
+        lib.fd2_sg_default_config(ctypes.byref(c))
+        c.device, c.hidden, c.radial_bins, c.radial_max_um = device, hidden, radial_bins, radial_max_um
+        c.batch, c.lr, c.radial_weight, c.seed = batch, lr, radial_weight, seed
+        self.config = c
+        self.radial_bins = radial_bins
+        self.radial_max_um = radial_max_um
+        self._h = ctypes.c_void_p()
+        check(lib.fd2_sg_create(ctypes.byref(c), ctypes.byref(self._h)), "fd2_sg_create")
+
+    def close(self):
+        if self._h:
+            self._lib.fd2_sg_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, where):
+        if st != _lib.OK:
+            raise _lib.Fd2Error(st, where, self._lib.fd2_sg_last_error(self._h).decode(errors="replace"))
+
+    def set_data(self, feats, photons, detected, radial, n_val: int = 0):
+        f = np.ascontiguousarray(feats, np.float32)
+        p = np.ascontiguousarray(photons, np.int32)
+        d = np.ascontiguousarray(detected, np.int32)
+        r = np.ascontiguousarray(radial, np.uint32)
+        self._check(self._lib.fd2_sg_set_data(self._h, ptr(f), ptr(p), ptr(d), ptr(r), len(p), n_val), "set_data")
+
+    def train(self, steps: int):
+        tl, vl = ctypes.c_float(), ctypes.c_float()
+        self._check(self._lib.fd2_sg_train(self._h, steps, ctypes.byref(tl), ctypes.byref(vl)), "train")
+        return float(tl.value), float(vl.value)
+
+    def eval(self) -> dict:
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        self._check(self._lib.fd2_sg_eval(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "eval")
+        return {"loss": a.value, "det_loss": b.value, "radial_loss": c.value}
+
+    def num_params(self) -> int:
+        return int(self._lib.fd2_sg_num_params(self._h))
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.num_params(), np.float32)
+        self._check(self._lib.fd2_sg_get_params(self._h, ptr(out), out.size), "get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self._lib.fd2_sg_set_params(self._h, ptr(p), p.size), "set_params")
+
+    def hull(self):
+        h = SgHull()
+        self._check(self._lib.fd2_sg_get_hull(self._h, ctypes.byref(h)), "get_hull")
+        return np.array(h.lo[:], np.float32), np.array(h.hi[:], np.float32)
+
+    def set_hull(self, lo, hi):
+        h = SgHull()
+        h.lo[:] = [float(v) for v in lo]
+        h.hi[:] = [float(v) for v in hi]
+        self._check(self._lib.fd2_sg_set_hull(self._h, ctypes.byref(h)), "set_hull")
+
+    def save(self, path: str):
+        self._check(self._lib.fd2_sg_save(self._h, path.encode()), "save")
+
+    def load(self, path: str):
+        self._check(self._lib.fd2_sg_load(self._h, path.encode()), "load")
+
+    def loss_grad(self, feats, photons, detected, radial):
+        f = np.ascontiguousarray(feats, np.float32)
+        p = np.ascontiguousarray(photons, np.int32)
+        d = np.ascontiguousarray(detected, np.int32)
+        r = np.ascontiguousarray(radial, np.uint32)
+        loss = ctypes.c_float()
+        g = np.zeros(self.num_params(), np.float32)
+        self._check(self._lib.fd2_sg_loss_grad(self._h, ptr(f), ptr(p), ptr(d), ptr(r), len(p), ctypes.byref(loss),
+                                               ptr(g)), "loss_grad")
+        return float(loss.value), g
+
+    def predict(self, feats) -> np.ndarray:
+        f = np.ascontiguousarray(feats, np.float32)
+        out = np.zeros((len(f), N_OUTPUTS), np.float32)
+        self._check(self._lib.fd2_sg_predict(self._h, ptr(f), len(f), ptr(out)), "predict")
+        return out
+
+    def run(self, transport: OpticalTransport, audit_fraction: float = 0.01) -> dict:
+        st = SgStats()
+        self._check(self._lib.fd2_sg_run(self._h, transport.handle, audit_fraction, ctypes.byref(st)), "run")
+        return st.as_dict()

@@ -1,0 +1,65 @@
+"""Train the surrogate on Monte Carlo labels: ``python -m hybridmantis_b200.train_surrogate``.
+
+Defaults follow the surrogate-training workload: 2,000,000 points over
+detector geometries drawn from the batched workload's ranges (thickness
+100-600 um, column radius 2.5-7.5 um, roughness 0-0.5, top reflectivity 0-1,
+bulk absorption 1e-5..1e-3 /um), each point a deposition at depth U(0, H)
+with energy U(1, 80) keV labelled by 10,000 Monte Carlo photons (detected
+fraction and a 64-bin radial histogram to 200 um); MLP 8-256-256-256-25,
+BF16 GEMMs with FP32 accumulation, Adam, batch 8,192, 5 % held out.
+Prints one JSON line with the losses and timings; writes the network with
+``--out``.
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import surrogate as sgm
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--geometries", type=int, default=1024)
+    ap.add_argument("--points", type=int, default=2_000_000)
+    ap.add_argument("--photons", type=int, default=10_000)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--val", type=float, default=0.05)
+    ap.add_argument("--seed", type=int, default=20240)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default="")
+    a = ap.parse_args()
+    t0 = time.perf_counter()
+    geoms = sgm.sample_geometries(a.geometries, seed=a.seed)
+    per = max(1, a.points // a.geometries)
+    f, ph, det, rad = sgm.label_points(geoms, per, a.photons, seed=a.seed + 1, device=a.device)
+    t_label = time.perf_counter() - t0
+    perm = np.random.default_rng(a.seed + 2).permutation(len(f))
+    f, ph, det, rad = f[perm], ph[perm], det[perm], rad[perm]
+    n_val = int(a.val * len(f))
+    with sgm.Surrogate(device=a.device, batch=a.batch, lr=a.lr, seed=a.seed + 3) as s:
+        s.set_data(f, ph, det, rad, n_val=n_val)
+        before = s.eval()
+        t1 = time.perf_counter()
+        curve = []
+        done = 0
+        while done < a.steps:
+            k = min(500, a.steps - done)
+            tl, vl = s.train(k)
+            done += k
+            curve.append({"step": done, "train": tl, "val": vl})
+        t_train = time.perf_counter() - t1
+        after = s.eval()
+        if a.out:
+            s.save(a.out)
+    print(json.dumps({"points": len(f), "photons_per_point": a.photons, "geometries": a.geometries,
+                      "label_s": t_label, "label_photons_per_s": float(np.sum(ph)) / t_label,
+                      "train_s": t_train, "steps": a.steps, "batch": a.batch,
+                      "val_before": before, "val_after": after, "curve": curve}))
+
+
+if __name__ == "__main__":
+    main()

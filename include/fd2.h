@@ -125,7 +125,12 @@ typedef struct fd2_options {
                                       random numbers as in the unsharded run     */
     int32_t fresnel_batch;         /* lanes parked at a column wall before the warp
                                       runs their Fresnel interaction; 0 = tuned   */
-    int32_t reserved;
+    int32_t radial_bins;           /* > 0: label mode -- each history's detected
+                                      photons are binned by distance from their
+                                      event in radial_bins bins up to
+                                      radial_max_um plus one overflow bin
+                                      (fd2_get_radial) instead of the PRF image */
+    double radial_max_um;
 } fd2_options;
 
 typedef struct fd2_counters {
@@ -196,6 +201,10 @@ FD2_API fd2_status fd2_get_prf_dims(fd2_ctx *ctx, int32_t geom, int32_t *xdim, i
 FD2_API fd2_status fd2_get_prf(fd2_ctx *ctx, int32_t geom, uint64_t *image, int64_t n);
 /* Detected photons per history, index hist - 1. */
 FD2_API fd2_status fd2_get_detected_per_primary(fd2_ctx *ctx, int32_t *counts, int64_t n);
+/* Label mode (options.radial_bins > 0): counts[h * (radial_bins + 1) + b]
+ * for history h (0-based) and radial bin b (the last is the overflow);
+ * n >= num_hist * (radial_bins + 1).  Surrogate training labels. */
+FD2_API fd2_status fd2_get_radial(fd2_ctx *ctx, uint32_t *counts, int64_t n);
 FD2_API fd2_status fd2_get_photon_counts(fd2_ctx *ctx, int32_t *nphot, int64_t n);
 FD2_API fd2_status fd2_get_phs(fd2_ctx *ctx, int32_t geom, int32_t *bins, int32_t num_bins);
 FD2_API fd2_status fd2_get_phs_stats(fd2_ctx *ctx, int32_t geom, fd2_phs_stats *out);

@@ -22,6 +22,12 @@
  *     the GPU: there is no CPU transport in this library -- and adds its
  *     PRF, PHS and counters into the COMMON blocks before returning, as
  *     the reference's CPU path does per call (c:342-372).
+ *   gpuoptlb_(gptime, lbbuf)         main/hybridMANTIS_cuda_ver1_0_LB.cu:108
+ *   cpuoptlb_(cptime, cpubufsize)    main/hybridMANTIS_c_ver1_0_LB.c:86
+ *     load-balancing probes (tally.f:198-210): transport optical_ events
+ *     [0, *lbbuf) (resp. [0, *cpubufsize)) synchronously -- both on the
+ *     GPU -- add the results into the COMMON blocks and return the elapsed
+ *     seconds in *gptime (resp. *cptime).
  */
 #ifndef FD2_COMPAT_H
 #define FD2_COMPAT_H
@@ -62,6 +68,8 @@ struct fd2_common_outputimage {
 
 FD2_API void gpuoptical_(int *penctr, int *myfactGPU);
 FD2_API void cpuoptical_(int *gpusize);
+FD2_API void gpuoptlb_(double *gptime, int *lbbuf);
+FD2_API void cpuoptlb_(double *cptime, int *cpubufsize);
 
 /* Status of the last shim call (the shims return void, as the reference's). */
 FD2_API fd2_status fd2_compat_status(void);

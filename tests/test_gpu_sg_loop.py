@@ -1,0 +1,93 @@
+"""The surrogate in the event pipeline (fd2_sg_run) against the plain Monte Carlo.
+
+A surrogate trained on Monte Carlo labels of the benchmark's 150 um detector
+replaces the transport of the same seeded 25 keV pencil-beam events: the
+per-x-ray detected counts (PHS mean, Swank factor) and the radial PRF must
+agree with a full Monte Carlo run of the same events within the accuracy a
+short training reaches, the bookkeeping must be consistent, and the audit
+must report its comparison.
+"""
+import numpy as np
+import pytest
+
+import hybridmantis_b200 as hb
+from hybridmantis_b200 import surrogate as sgm
+
+from gpu_helpers import report
+from mcstats import phs_moments, radial_profile
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def trained(require_gpu):
+    es = hb.synth_events(0, 600, 41)
+    g = hb.params_to_geometry(es.params)
+    f, ph, det, rad = sgm.label_points([g], 6144, 2000, seed=42, energy_kev=(0.5, 30.0))
+    s = sgm.Surrogate(hidden=256, batch=2048, lr=2e-3, seed=43)
+    s.set_data(f, ph, det, rad, n_val=512)
+    s.train(1500)
+    yield s, es
+    s.close()
+
+
+def _run(es, sg=None, audit=0.0):
+    with hb.OpticalTransport(es.params, count_mode=hb.COUNT_GAUSSIAN, seed=99) as t:
+        t.submit(es)
+        stats = None
+        if sg is None:
+            t.run_sync()
+        else:
+            stats = sg.run(t, audit)
+        return {"counters": t.counters(), "prim": t.detected_per_primary(), "prf": t.prf(), "stats": stats,
+                "counts": t.photon_counts(es.n)}
+
+
+def test_surrogate_run_matches_monte_carlo(trained):
+    sg, es = trained
+    mc = _run(es)
+    sr = _run(es, sg, audit=0.1)
+    st = sr["stats"]
+    # every event with photons went one way or the other; same photon counts
+    n_with = int(np.count_nonzero(mc["counts"]))
+    assert st["surrogate_events"] + st["mc_events"] == n_with
+    assert np.array_equal(sr["counts"], mc["counts"])
+    assert st["surrogate_events"] >= 0.9 * n_with
+    assert st["audit_events"] > 0
+    # bookkeeping: the detected counter equals the per-history counts
+    assert sr["counters"]["detected"] == int(sr["prim"].sum())
+    assert sr["counters"]["generated"] == mc["counters"]["generated"]
+    # PHS statistics
+    a, b = phs_moments(sr["prim"]), phs_moments(mc["prim"])
+    rep = {"sg": a, "mc": b, "stats": st}
+    assert abs(a["mean"] - b["mean"]) <= 0.03 * b["mean"], rep
+    assert abs(a["swank"] - b["swank"]) <= 0.01, rep
+    # radial PRF profile (normalised), L1 distance
+    edges = np.array([0, 1, 2, 3, 4, 6, 8, 11, 15, 20, 30, 45, 70, 110, 170, 260, 400])
+    rs = radial_profile(sr["prf"], 250.5, 250.5, edges).astype(np.float64)
+    rm = radial_profile(mc["prf"], 250.5, 250.5, edges).astype(np.float64)
+    l1 = np.abs(rs / rs.sum() - rm / rm.sum()).sum()
+    rep["radial_l1"] = l1
+    report("surrogate_loop_c0", rep)
+    assert l1 < 0.06, rep
+    # audit: the Monte Carlo of the audited events agrees with the prediction
+    assert abs(st["audit_z"]) < 6.0 or abs(st["audit_mc_detected"] - st["audit_sg_expected"]) \
+        <= 0.03 * st["audit_mc_detected"], rep
+    assert st["audit_radial_l1"] < 0.1, rep
+
+
+def test_out_of_hull_events_use_monte_carlo(trained):
+    sg, es = trained
+    lo, hi = sg.hull()
+    # a hull no event's energy reaches: all Monte Carlo, identical to fd2_run
+    lo2, hi2 = lo.copy(), hi.copy()
+    lo2[1], hi2[1] = 1e6, 2e6
+    sg.set_hull(lo2, hi2)
+    try:
+        sr = _run(es, sg, audit=0.0)
+    finally:
+        sg.set_hull(lo, hi)
+    mc = _run(es)
+    assert sr["stats"]["surrogate_events"] == 0
+    assert np.array_equal(sr["prim"], mc["prim"])
+    assert np.array_equal(sr["prf"], mc["prf"])

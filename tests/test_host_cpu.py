@@ -22,7 +22,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def declared_symbols():
     names = set()
-    for h in ("fd2.h", "fd2_compat.h"):
+    for h in sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")):
         text = open(os.path.join(ROOT, "include", h)).read()
         for m in re.finditer(r"FD2_API\s+[\w\s\*]+?\b(\w+)\s*\(", text):
             names.add(m.group(1))
