@@ -67,16 +67,16 @@ __device__ __forceinline__ float u01(uint32_t r)
     return __uint_as_float(0x3F800000u | (r >> 9)) - 0.99999994039535522461f;
 }
 
-constexpr int kURing = 32;     // uniforms buffered per lane
-constexpr int kURingLow = 12; // a lane at or below this level must generate
+constexpr int kURing = 32;      // uniforms buffered per lane
+constexpr int kURingLow = 12;  // inside a step: a lane at or below this level must generate
+constexpr int kURingStep = 24; // at a step's start the warp generates while a lane is at or below this
 
 // Internal step result: the photon waits at a column wall for the Fresnel
 // part of its surface interaction (not a fate).
 constexpr int kNeedsFresnel = 100;
 
-// Warp-uniform part of a Philox stream: the round keys of the run seed,
-// read where the kernel keeps them (its __grid_constant__ parameters, so
-// the rounds take them as constant-bank operands), and the run counter.
+// Warp-uniform part of a Philox stream: the round keys of the run seed
+// (the kernel keeps them in shared memory) and the run counter.
 struct RngKey {
     const uint32_t *rk;
     uint32_t run;
@@ -122,6 +122,28 @@ __device__ __forceinline__ float wall_root(float qa, float qb, float qc)
     return (s - qb) / (2.0f * qa);
 }
 
+struct RefillState {
+    uint32_t tail, block;
+};
+
+// Refill inside a step: rarely taken once the step start leaves every ring
+// above kURingStep, so it is one out-of-line copy instead of an inlined
+// Philox at every loop of the walk (the walk's code then stays small enough
+// for the instruction cache).  Fills the lane's ring completely.
+__device__ __noinline__ RefillState refill_slow(float *ring, int stride, uint32_t head, uint32_t tail, uint32_t block,
+                                               uint32_t photon, uint32_t event, uint32_t run, const uint32_t *rk)
+{
+    while (tail - head <= (uint32_t)(kURing - 4)) {
+        const uint4 r = philox4x32_10_rk(make_uint4(block++, photon, event, run), rk);
+        ring[((tail + 0) & (kURing - 1)) * stride] = u01(r.x);
+        ring[((tail + 1) & (kURing - 1)) * stride] = u01(r.y);
+        ring[((tail + 2) & (kURing - 1)) * stride] = u01(r.z);
+        ring[((tail + 3) & (kURing - 1)) * stride] = u01(r.w);
+        tail += 4;
+    }
+    return {tail, block};
+}
+
 struct Walker {
     // photon
     float px, py, pz;   // position
@@ -132,13 +154,14 @@ struct Walker {
     float dist;         // path length
     uint32_t rebound;   // boundary interactions
     int ii, jj;         // detection pixel (-1: outside the PRF bounds)
-    // Philox stream of the photon and the lane's uniform ring.  The ring is
-    // topped up to at least kURingLow + 1 = 13 uniforms at the start of every
-    // step, loop iteration and new-normal attempt; no segment between two
-    // top-ups draws more than 7, so a draw is a plain shared-memory load.
-    // `underflow` records a draw from an empty ring (never expected;
-    // reported).  Generating ahead does not change the values a photon
-    // draws: its stream is consumed in counter order either way.
+    // Philox stream of the photon and the lane's uniform ring.  At the start
+    // of a step the warp tops every ring up above kURingStep (top_up); at
+    // every loop iteration and new-normal attempt inside the step a ring at
+    // or below kURingLow is refilled out of line (top_up_inner).  No segment
+    // between two checks draws more than 7, so a draw is a plain
+    // shared-memory load.  `underflow` records a draw from an empty ring
+    // (never expected; reported).  Generating ahead does not change the
+    // values a photon draws: its stream is consumed in counter order.
     float *ring;
     int stride;
     uint32_t head, tail, block, photon, event;
@@ -149,7 +172,7 @@ struct Walker {
     {
         const unsigned mask = __activemask();
 #pragma unroll 1
-        while (__any_sync(mask, tail - head <= (uint32_t)kURingLow)) {
+        while (__any_sync(mask, tail - head <= (uint32_t)kURingStep)) {
             if (tail - head <= (uint32_t)(kURing - 4)) {
                 const uint4 r = philox4x32_10_rk(make_uint4(block++, photon, event, key.run), key.rk);
                 ring[((tail + 0) & (kURing - 1)) * stride] = u01(r.x);
@@ -158,6 +181,16 @@ struct Walker {
                 ring[((tail + 3) & (kURing - 1)) * stride] = u01(r.w);
                 tail += 4;
             }
+        }
+    }
+    // Inside a step: keep at least kURingLow + 1 uniforms (no segment between
+    // two calls draws more than 7).
+    __device__ __forceinline__ void top_up_inner()
+    {
+        if (tail - head <= (uint32_t)kURingLow) {
+            const RefillState r = refill_slow(ring, stride, head, tail, block, photon, event, key.run, key.rk);
+            tail = r.tail;
+            block = r.block;
         }
     }
     __device__ __forceinline__ float u()
@@ -190,7 +223,7 @@ struct Walker {
         float c = 2.0f * u() - 1.0f;
         if (first) {
             for (int t = 0; t < 64 && fabsf(c) <= 0.01f; ++t) {
-                top_up();
+                top_up_inner();
                 c = 2.0f * u() - 1.0f;
             }
         }
@@ -308,7 +341,7 @@ struct Walker {
                                                      bool always_rough)
     {
         for (;;) {
-            top_up();
+            top_up_inner();
             nx = ix; ny = iy; nz = iz;
             roughen(1.0f);
             const float inv = rsqrtf(nx * nx + ny * ny);
@@ -362,7 +395,7 @@ struct Walker {
         int tries = 0, tries_top = 0;
         bool hop = !crosstalk, side_hop = true;
         for (int loop = 0; loop < kMaxTopLoops; ++loop) {
-            top_up();
+            top_up_inner();
             bool sensor_hit = false;
             if (hop) {
                 const float sx = px, sy = py, sz = pz;
@@ -416,7 +449,7 @@ struct Walker {
             // top reflector / sensor at the end of the hop
             bool again = false;
             for (int k = 0; k < kMaxTopLoops; ++k) {
-                top_up();
+                top_up_inner();
                 if (at_top(g)) {
                     if (g.top_absfrac > 0.0f && u() < g.top_absfrac) return kAbsTop;
                     dz = -fabsf(2.0f * u() - 1.0f);
@@ -492,7 +525,7 @@ struct Walker {
         enum { kLeave, kNewSurface, kRestore, kIncidence } stage = kNewSurface;
         int fate = kAlive;
         for (int loop = 0; loop < kMaxSurfaceLoops; ++loop) {
-            top_up();
+            top_up_inner();
             if (stage == kNewSurface) {
                 if (!outside) {
                     const float ax = xc - px, ay = yc - py;

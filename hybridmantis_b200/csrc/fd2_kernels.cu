@@ -363,13 +363,18 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     bool exhausted = false, alive = false, parked = false;
     const unsigned refill_min = (unsigned)a.refill;
     const unsigned fresnel_min = (unsigned)max(a.fresnel_batch, 1);
+    // Philox round keys and run counter, shared by the CTA
+    __shared__ uint32_t s_rk[20];
+    __shared__ uint32_t s_run;
+    if (threadIdx.x < 20) s_rk[threadIdx.x] = a.round_keys[threadIdx.x];
+    if (threadIdx.x == 0) s_run = *a.run_tag;
 
     __syncthreads();
     Walker w;
     w.ring = s_uring + threadIdx.x;
     w.stride = blockDim.x;
-    w.key.rk = a.round_keys;
-    w.key.run = *a.run_tag;
+    w.key.rk = s_rk;
+    w.key.run = s_run;
     int prim = 0, geom = 0;
 
     for (;;) {

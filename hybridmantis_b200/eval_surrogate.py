@@ -1,0 +1,100 @@
+"""Surrogate in the loop against the plain Monte Carlo on the same events:
+``python -m hybridmantis_b200.eval_surrogate --model FILE``.
+
+Transports one seeded synthetic stream twice through the same context
+settings -- once with fd2_run (Monte Carlo), once with fd2_sg_run -- and
+prints one JSON line: x-rays/s of both, PHS mean and Swank factor of both,
+the L1 distance of their normalised radial PRF profiles and of their
+normalised PRF images, and the audit statistics.  Default stream: 1,000,000
+x-rays, triangular 20-70 keV, 500 um CsI, R = 5 um, clusters as the
+benchmark workload (the surrogate-in-the-loop configuration).
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import fastdetect2 as fd
+from . import surrogate as sgm
+
+
+def _moments(prim):
+    c = np.asarray(prim, np.float64)
+    c = c[c > 0]
+    m1, m2 = c.mean(), (c * c).mean()
+    return float(m1), float(m1 * m1 / m2)
+
+
+def _radial(img, cx, cy, edges):
+    img = np.asarray(img, np.float64)
+    ii, jj = np.meshgrid(np.arange(img.shape[0]) + 0.5, np.arange(img.shape[1]) + 0.5, indexing="ij")
+    r = np.hypot(ii - cx, jj - cy)
+    h = np.histogram(r.ravel(), bins=edges, weights=img.ravel())[0]
+    return h / max(h.sum(), 1.0)
+
+
+def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 4242, audit: float = 0.01,
+             device: int = 0, repeats: int = 2) -> dict:
+    es = fd.synth_events(config, xrays, seed)
+    out = {"config": config, "xrays": es.params.num_hist, "events": es.n}
+    res = {}
+    with sgm.Surrogate(device=device) as s:
+        s.load(model)
+        for mode in ("mc", "sg"):
+            with fd.OpticalTransport(es.params, device=device, seed=seed + 1) as t:
+                t.submit(es)
+                # warm-up run, then timed runs on reset tallies
+                if mode == "mc":
+                    t.run_sync()
+                else:
+                    s.run(t, audit)
+                times = []
+                stats = None
+                for _ in range(repeats):
+                    t.reset_tallies()
+                    t0 = time.perf_counter()
+                    if mode == "mc":
+                        t.run_sync()
+                    else:
+                        stats = s.run(t, audit)
+                    times.append(time.perf_counter() - t0)
+                prim = t.detected_per_primary()
+                img = t.prf().astype(np.float64)
+                c = t.counters()
+            mean, swank = _moments(prim)
+            res[mode] = {"seconds": min(times), "xrays_per_s": es.params.num_hist / min(times), "phs_mean": mean,
+                         "swank": swank, "detected": c["detected"], "image": img, "stats": stats}
+    edges = np.array([0, 1, 2, 3, 4, 6, 8, 11, 15, 20, 30, 45, 70, 110, 170, 260, 400])
+    cx = float(np.mean(es.x_um)) - es.params.lb_x
+    cy = float(np.mean(es.y_um)) - es.params.lb_y
+    rm, rs = _radial(res["mc"]["image"], cx, cy, edges), _radial(res["sg"]["image"], cx, cy, edges)
+    im, isg = res["mc"]["image"], res["sg"]["image"]
+    out.update({
+        "mc_xrays_per_s": res["mc"]["xrays_per_s"], "sg_xrays_per_s": res["sg"]["xrays_per_s"],
+        "speedup": res["sg"]["xrays_per_s"] / res["mc"]["xrays_per_s"],
+        "mc_seconds": res["mc"]["seconds"], "sg_seconds": res["sg"]["seconds"],
+        "phs_mean": [res["mc"]["phs_mean"], res["sg"]["phs_mean"]],
+        "swank": [res["mc"]["swank"], res["sg"]["swank"]],
+        "swank_diff": res["sg"]["swank"] - res["mc"]["swank"],
+        "radial_prf_l1": float(np.abs(rm - rs).sum()),
+        "prf_image_l1": float(np.abs(im / im.sum() - isg / isg.sum()).sum()),
+        "detected": [res["mc"]["detected"], res["sg"]["detected"]],
+        "sg_stats": res["sg"]["stats"],
+    })
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--model", required=True)
+    ap.add_argument("--config", type=int, default=4)
+    ap.add_argument("--xrays", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=4242)
+    ap.add_argument("--audit", type=float, default=0.01)
+    a = ap.parse_args()
+    print(json.dumps(evaluate(a.model, a.config, a.xrays, a.seed, a.audit)))
+
+
+if __name__ == "__main__":
+    main()
