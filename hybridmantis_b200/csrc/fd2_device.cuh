@@ -74,6 +74,11 @@ constexpr int kURingStep = 24; // at a step's start the warp generates while a l
 // Internal step result: the photon waits at a column wall for the Fresnel
 // part of its surface interaction (not a fate).
 constexpr int kNeedsFresnel = 100;
+// Internal step results of the crosstalk path: the photon crosses into the
+// adjacent column and needs that column's normal (crosstalk_normal), or its
+// attempt was rejected and is retried in the next round.
+constexpr int kNeedsNormal = 101;
+constexpr int kRetryNormal = 102;
 
 // Warp-uniform part of a Philox stream: the round keys of the run seed
 // (the kernel keeps them in shared memory) and the run counter.
@@ -384,20 +389,20 @@ struct Walker {
         return new_column_normal(g, ix, iy, iz, tries, true);
     }
 
-    // Leave the current column (transmit): cross into the adjacent column
-    // (crosstalk), or hop U(d_min, d_max) with the top reflector and the
-    // sensor on the way, then orient the next column.  Hops after a top
-    // reflection repeat the loop.
+    // Leave the current column after a transmission through its wall
+    // (transmit without crosstalk; crosstalk is crosstalk_normal): hop
+    // U(d_min, d_max) with the top reflector and the sensor on the way, then
+    // orient the next column.  Hops after a top reflection repeat the loop.
     template <class G>
-    __device__ __forceinline__ int leave_column(const G &g, bool crosstalk)
+    __device__ __forceinline__ int leave_column(const G &g)
     {
         float ix = -dx, iy = -dy, iz = -dz;
         int tries = 0, tries_top = 0;
-        bool hop = !crosstalk, side_hop = true;
+        bool side_hop = true;
         for (int loop = 0; loop < kMaxTopLoops; ++loop) {
             top_up_inner();
             bool sensor_hit = false;
-            if (hop) {
+            {
                 const float sx = px, sy = py, sz = pz;
                 const float d = fmaf(u(), g.d_span, g.d_min);
                 px = fmaf(dx, d, sx);
@@ -441,7 +446,6 @@ struct Walker {
             if (!up_to_top) {
                 const int f = new_column_normal(g, ix, iy, iz, side_hop ? tries : tries_top, false);
                 if (f != kAlive) return f;
-                if (crosstalk) return kAlive;
                 if (side_hop && (fabsf(px) < kEps || fabsf(px - g.xdet) < kEps || fabsf(py) < kEps ||
                                  fabsf(py - g.ydet) < kEps))
                     return kLost;
@@ -474,7 +478,6 @@ struct Walker {
                 if (!at_top(g)) return kAlive;
             }
             if (!again) return kCapped;
-            hop = true;
             side_hop = false;
         }
         return kCapped;
@@ -505,11 +508,36 @@ struct Walker {
         else if (pz < g.cct_band_lo && pz >= 0.0f) cct = fmaf(pz, g.cct_k_hi, 0.5f);
         else if (pz < 0.0f && pz >= -g.half) cct = fmaf(pz + g.half, g.cct_k_lo, 1.0f);
         if (!(u() < cct)) return kNeedsFresnel;
-        const int f = leave_column(g, true);
-        if (f != kAlive) return f;
-        xc = fmaf(-g.R, nx, px);
-        yc = fmaf(-g.R, ny, py);
-        return kAlive;
+        return kNeedsNormal;
+    }
+
+    // Crosstalk into the adjacent column (transmit with crosstalk): one
+    // attempt at the new column's normal, a random normal within 1.57 rad of
+    // the reversed direction, flattened and roughened.  Returns kAlive (the
+    // photon is in the new column), kTheta1 (no normal after 100 retries) or
+    // kRetryNormal (rejected: the kernel retries in its next round, beside
+    // the other lanes' first attempts, instead of looping here with the few
+    // rejected lanes of the warp).
+    template <class G>
+    __device__ __forceinline__ int crosstalk_normal(const G &g, int &tries)
+    {
+        top_up_inner();
+        const float ix = -dx, iy = -dy, iz = -dz;
+        nx = ix; ny = iy; nz = iz;
+        roughen(1.0f);
+        const float inv = rsqrtf(nx * nx + ny * ny);
+        nx *= inv; ny *= inv; nz = 0.0f;
+        if (g.beta > 0.0f) roughen(g.beta);
+        if (!(ix * nx + iy * ny + iz * nz < kCos157)) {
+            xc = fmaf(-g.R, nx, px);
+            yc = fmaf(-g.R, ny, py);
+            return kAlive;
+        }
+        if (tries < 100) {
+            ++tries;
+            return kRetryNormal;
+        }
+        return kTheta1;
     }
 
     // Second part: Fresnel reflection / refraction on the rough wall, with
@@ -622,7 +650,7 @@ struct Walker {
                 }
             }
             // kLeave: hop between columns
-            const int f = leave_column(g, false);
+            const int f = leave_column(g);
             if (f != kAlive) {
                 fate = f;
                 break;

@@ -361,6 +361,8 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     int ring_len = 0, slot = 0, refills = 0;
     uint32_t used = 0;
     bool exhausted = false, alive = false, parked = false;
+    bool xretry = false;  // the lane's crosstalk normal is retried this round
+    int xtries = 0;
     const unsigned refill_min = (unsigned)a.refill;
     const unsigned fresnel_min = (unsigned)max(a.fresnel_batch, 1);
     // Philox round keys and run counter, shared by the CTA
@@ -453,10 +455,20 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         // them wait (or nothing else runs)
         int fate = kAlive;
         if (alive && !parked) {
-            fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
-            if (fate == kNeedsFresnel) {
-                parked = true;
-                fate = kAlive;
+            if (!xretry) {
+                fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
+                if (fate == kNeedsFresnel) {
+                    parked = true;
+                    fate = kAlive;
+                }
+            }
+            // crosstalk: one attempt at the next column's normal per round, so
+            // a rejected attempt is retried beside the other lanes' first ones
+            if (xretry || fate == kNeedsNormal) {
+                fate = kMulti ? w.crosstalk_normal(s_geom[geom], xtries) : w.crosstalk_normal(a.g0, xtries);
+                xretry = fate == kRetryNormal;
+                if (xretry) fate = kAlive;
+                else xtries = 0;
             }
         }
         const unsigned waiting = __ballot_sync(kFull, parked);
@@ -654,11 +666,25 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
 
 cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
 {
-    const int bytes = (int)transport_smem_bytes(cfg, n_geom);
-    cudaError_t e = cudaSuccess;
-#define FD2_SET_ATTR(M, T, B, R)                                                                                \
-    if (e == cudaSuccess)                                                                                       \
-        e = cudaFuncSetAttribute(transport_kernel<M, T, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    // The attribute is global to each kernel, shared by every context of the
+    // process, so it is set to the device's opt-in maximum (a launch only
+    // reserves what it asks for): contexts with different shared-memory
+    // needs cannot undo each other's setting.
+    int dev = 0, max_optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    const size_t need = transport_smem_bytes(cfg, n_geom);
+    // dynamic limit = opt-in maximum - the kernel's static shared memory
+#define FD2_SET_ATTR(M, T, B, R)                                                                          \
+    if (e == cudaSuccess) {                                                                               \
+        cudaFuncAttributes fa;                                                                            \
+        e = cudaFuncGetAttributes(&fa, transport_kernel<M, T, B, R>);                                     \
+        const int lim = max_optin - (int)fa.sharedSizeBytes;                                              \
+        if (e == cudaSuccess && need > (size_t)lim) e = cudaErrorInvalidValue;                            \
+        if (e == cudaSuccess)                                                                             \
+            e = cudaFuncSetAttribute(transport_kernel<M, T, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim); \
+    }
     FD2_TRANSPORT_VARIANTS(FD2_SET_ATTR)
 #undef FD2_SET_ATTR
     return e;

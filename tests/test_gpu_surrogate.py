@@ -120,3 +120,18 @@ def test_training_beats_constant_predictor(require_gpu, tmp_path):
         s2.load(path)
         assert np.array_equal(s2.params(), params)
         assert np.allclose(s2.predict(f[-n_val:]), out, atol=1e-5)
+
+
+def test_contexts_with_different_shared_memory_alternate(require_gpu):
+    """A label-mode context (no PRF window) created between two runs of an
+    ordinary one (a shared-memory PRF window) must not break the latter:
+    the kernels' shared-memory limit is process-wide."""
+    es = hb.synth_events(0, 40, 3)
+    with hb.OpticalTransport(es.params, seed=1) as t:
+        t.submit(es)
+        t.run_sync()
+        first = t.counters()["generated"]
+        geoms = sgm.sample_geometries(1, seed=2)
+        sgm.label_points(geoms, 16, 500, seed=3)
+        t.run_sync()
+        assert t.counters()["generated"] > first
