@@ -16,6 +16,11 @@ photon counts ~ Poisson(E * 54/keV) sampled on the GPU each step.
   reference_gpu the reference's own CUDA kernel `algo` (oracle/_ref,
           compiled for sm_100a with its own flags) on the same events and
           photon counts, one launch of its 18000 x 128 grid
+  surrogate  x-rays/s of the surrogate in the loop (fd2_sg_run, trained
+          network in hybridmantis_b200/data) against the plain Monte Carlo on
+          the same 1,000,000-x-ray, 500 um stream, with the PHS/Swank and PRF
+          errors between the two and the same errors between two Monte Carlo
+          runs (the noise floor)
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU: one rank per GPU (torchrun); each rank transports its own x-ray
@@ -75,6 +80,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--surrogate-model", default=os.path.join(ROOT, "hybridmantis_b200", "data", "surrogate_c4.fd2sg"))
+    ap.add_argument("--surrogate-xrays", type=int, default=1_000_000)
+    ap.add_argument("--no-surrogate", action="store_true")
     return ap.parse_args()
 
 
@@ -371,6 +379,22 @@ def run_ours(a, rank, world, local_rank):
         ref_gpu = None
         if not a.no_ref_gpu and world == 1:
             ref_gpu = reference_gpu(es, nphot, local_rank)
+        surrogate = None
+        if not a.no_surrogate and world == 1 and os.path.exists(a.surrogate_model):
+            from hybridmantis_b200 import eval_surrogate
+            ev = eval_surrogate.evaluate(a.surrogate_model, config=4, xrays=a.surrogate_xrays, seed=a.seed,
+                                         audit=0.01, device=local_rank, repeats=2, noise_floor=True)
+            st = ev.pop("sg_stats")
+            surrogate = {"metric": "x-rays/s", "value": ev["sg_xrays_per_s"], "mc_value": ev["mc_xrays_per_s"],
+                         "speedup_vs_mc": ev["speedup"],
+                         "workload": f"config 4: {ev['xrays']} x-rays, triangular 20-70 keV, 500 um CsI, R=5 um, "
+                                     f"clusters as config 1 ({ev['events']} events); same seeded stream for both",
+                         "phs_mean": ev["phs_mean"], "swank": ev["swank"], "swank_diff": ev["swank_diff"],
+                         "radial_prf_l1": ev["radial_prf_l1"], "prf_image_l1": ev["prf_image_l1"],
+                         "mc_vs_mc": ev.get("mc_vs_mc"),
+                         "audit": {k: st[k] for k in ("audit_events", "audit_z", "audit_radial_l1", "audit_ms")},
+                         "mc_fallback_events": st["mc_events"], "surrogate_events": st["surrogate_events"],
+                         "model": os.path.relpath(a.surrogate_model, ROOT)}
         clocks = clk.summary()
         out = {
             "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": a.steps,
@@ -389,6 +413,7 @@ def run_ours(a, rank, world, local_rank):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
+            "surrogate": surrogate,
             "clocks": clocks,
             "results": {"phs_mean": stats["mean"], "swank": stats["swank"],
                         "fates_per_photon": {k: cnt[k] / max(cnt["generated"], 1) for k in

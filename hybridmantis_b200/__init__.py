@@ -8,3 +8,4 @@ from .fastdetect2 import (COUNT_GAUSSIAN, COUNT_GIVEN, COUNT_POISSON, REPLAY_FP6
                           EventSet, OpticalTransport, default_params, params_to_geometry, prf_dims,
                           read_events_binary, read_events_text, read_input_file, synth_events,
                           write_events_binary, write_events_text, write_output_files)
+from .surrogate import Surrogate  # noqa: F401,E402

@@ -102,7 +102,7 @@ class SgConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("hidden", ctypes.c_int32), ("radial_bins", ctypes.c_int32),
                 ("radial_max_um", ctypes.c_double), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
                 ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("adam_eps", ctypes.c_float),
-                ("radial_weight", ctypes.c_float), ("seed", ctypes.c_uint64)]
+                ("radial_weight", ctypes.c_float), ("lateral_um", ctypes.c_float), ("seed", ctypes.c_uint64)]
 
 
 class SgHull(ctypes.Structure):
@@ -135,7 +135,7 @@ EXPORTED = [
     "fd2_read_events_binary", "fd2_write_events_binary",
     "gpuoptical_", "cpuoptical_", "gpuoptlb_", "cpuoptlb_", "fd2_compat_status",
     "fd2_sg_default_config", "fd2_sg_create", "fd2_sg_destroy", "fd2_sg_last_error", "fd2_sg_set_data",
-    "fd2_sg_train", "fd2_sg_eval", "fd2_sg_num_params", "fd2_sg_get_params", "fd2_sg_set_params",
+    "fd2_sg_train", "fd2_sg_set_lr", "fd2_sg_eval", "fd2_sg_num_params", "fd2_sg_get_params", "fd2_sg_set_params",
     "fd2_sg_get_hull", "fd2_sg_set_hull", "fd2_sg_save", "fd2_sg_load", "fd2_sg_loss_grad", "fd2_sg_predict",
     "fd2_sg_run",
 ]
@@ -199,6 +199,7 @@ def load():
         "fd2_sg_set_data": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_int64]),
         "fd2_sg_train": (ctypes.c_int, [vp, ctypes.c_int32, P(ctypes.c_float), P(ctypes.c_float)]),
         "fd2_sg_eval": (ctypes.c_int, [vp, P(ctypes.c_float), P(ctypes.c_float), P(ctypes.c_float)]),
+        "fd2_sg_set_lr": (ctypes.c_int, [vp, ctypes.c_float]),
         "fd2_sg_num_params": (ctypes.c_int64, [vp]),
         "fd2_sg_get_params": (ctypes.c_int, [vp, vp, ctypes.c_int64]),
         "fd2_sg_set_params": (ctypes.c_int, [vp, vp, ctypes.c_int64]),

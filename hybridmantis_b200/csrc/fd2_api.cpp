@@ -270,7 +270,7 @@ fd2::TransportArgs transport_args(fd2_ctx *c)
     a.status = c->d_flags;
     a.radial = c->d_radial;
     a.radial_bins = c->d_radial ? c->opt.radial_bins : 0;
-    a.radial_inv_width = c->d_radial ? (float)(c->opt.radial_bins / c->opt.radial_max_um) : 0.0f;
+    a.radial_inv_max = c->d_radial ? (float)(1.0 / c->opt.radial_max_um) : 0.0f;
     return a;
 }
 

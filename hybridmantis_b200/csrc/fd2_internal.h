@@ -49,7 +49,7 @@ struct TransportArgs {
     // label mode: per-history radial histograms of detected photons
     unsigned int *radial;        // [n_prim][radial_bins + 1], null = off
     int radial_bins;
-    float radial_inv_width;      // bins per micrometre
+    float radial_inv_max;        // 1 / r_max (bin j covers r_max (j/bins)^2 .. r_max ((j+1)/bins)^2)
 };
 
 // Device status bits (the `status` word).

@@ -501,7 +501,10 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                 const int ydim = kMulti ? s_geom[geom].ydim : a.g0.ydim;
                 if (kRadial) {
                     const float rx = w.px - w.ex, ry = w.py - w.ey;
-                    const int b = min((int)(sqrtf(rx * rx + ry * ry) * a.radial_inv_width), a.radial_bins);
+                    // quadratic edges: bin = floor(bins sqrt(r / r_max))
+                    const float rr = sqrtf(rx * rx + ry * ry) * a.radial_inv_max;
+                    const int b = rr < 1.0f ? min((int)(sqrtf(rr) * (float)a.radial_bins), a.radial_bins - 1)
+                                            : a.radial_bins;
                     if (prim < a.n_prim && b >= 0)
                         atomicAdd(&a.radial[(long long)prim * (a.radial_bins + 1) + b], 1u);
                 } else if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {

@@ -19,9 +19,18 @@ constexpr int kComponents = FD2_SG_COMPONENTS;
 constexpr int kInPad = 32;   // input width seen by the first GEMM (K multiple of 32)
 constexpr int kOutPad = 64;  // output width of the last GEMM
 constexpr int kMaxSplits = 16;
-constexpr float kMuScale = 50.0f;  // um per unit of the mean outputs
+constexpr float kMuScale = 50.0f;  // ring radius = kMuScale * softplus(output), um (>= 0)
 constexpr float kSdScale = 10.0f;  // um
 constexpr float kLogSdMin = -6.0f, kLogSdMax = 4.0f;
+
+// Radial categories: bin j < bins covers [e_j, e_{j+1}) with quadratic edges
+// e_j = r_max (j / bins)^2 (fine near the deposition, where the column wall
+// shapes the profile); category `bins` is r >= r_max.
+__host__ __device__ inline float radial_edge(int j, int bins, float r_max)
+{
+    const float t = (float)j / (float)bins;
+    return r_max * t * t;
+}
 
 // parameter blocks of the FP32 master vector
 enum { kW1 = 0, kB1, kW2, kB2, kW3, kB3, kW4, kB4, kNumBlocks };
@@ -42,8 +51,11 @@ struct fd2_sg {
     int hidden = 256, bins = 64, batch = 8192;
     double radial_max = 200.0;
     float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f, lambda = 1.0f;
+    float lateral_um = 50.0f;
     uint64_t seed = 0;
-    fd2_sg_hull hull{};
+    fd2_sg_hull hull{};      // routing box: events outside go to the Monte Carlo
+    fd2_sg_hull norm_box{};  // input normalisation box, fixed by the first hull the network gets
+    bool norm_fixed = false;
     fd2::sg::NormParams norm{};
 
     // parameters (FP32 masters, gradients, Adam moments, BF16 copies)
@@ -54,6 +66,7 @@ struct fd2_sg {
     uint8_t *d_live = nullptr;
     unsigned long long *d_step = nullptr;
     double *d_acc = nullptr;
+    float *d_lr = nullptr;  // Adam step size (read by the captured step)
     float *ws = nullptr;  // split-K partials
 
     // activations for up to cap_rows rows

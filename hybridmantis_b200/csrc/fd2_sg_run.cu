@@ -12,7 +12,10 @@
 //      event, rows beyond the device-side row count skipped);
 //   5. sampling, one warp per row: detected count ~ Binomial(N, p) split over
 //      the 32 lanes (geometric skipping), then each detected photon's radius
-//      from the truncated mixture, a uniform azimuth, and the PRF pixel;
+//      drawn exactly from one ring of the mixture, an azimuth uniform over
+//      the directions that stay on the detector (the labels' depositions sit
+//      at the detector centre, so their far light is what the detector's
+//      edges leave), and the PRF pixel;
 //      per-history counts and counters as the Monte Carlo tallies them;
 //   6. PHS and the run counter (the context's last pipeline segment);
 //   7. audit: the audited rows' depositions are transported by the Monte
@@ -32,6 +35,7 @@
 #include "fd2_internal.h"
 #include "fd2_sg_gemm.cuh"
 #include "fd2_sg_internal.h"
+#include "fd2_sg_mix.cuh"
 #include "fd2_surrogate.h"
 
 using namespace fd2::sg;
@@ -45,11 +49,16 @@ struct RunBuffers {
     __nv_bfloat16 *x0 = nullptr, *ha = nullptr, *hb = nullptr;
     float *out = nullptr;
     unsigned long long *d_stat = nullptr;  // [0] surrogate photons, [1] detected
-    // audit gather (compact copies of the audited rows)
+    // audit: compact copies of the audited rows, pooled predictions
     float4 *a_pos = nullptr;
     int32_t *a_n = nullptr, *a_geom = nullptr;
-    float *a_out = nullptr;
+    double *a_pool = nullptr;  // [0, bins] sum N p q_j, then sum N p, sum N p (1 - p), sum N
     int64_t a_cap = 0;
+    // label-mode Monte Carlo context of the audit, kept across runs
+    fd2_ctx *audit = nullptr;
+    int32_t audit_cap = 0;
+    std::vector<fd2_geometry> audit_geoms;
+    fd2_params audit_params{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -59,8 +68,9 @@ void sg_free_run_buffers(fd2_sg *s)
     if (!r) return;
     for (void *p : {(void *)r->d_count, (void *)r->sg_event, (void *)r->sg_n, (void *)r->audit_row, (void *)r->x0,
                     (void *)r->ha, (void *)r->hb, (void *)r->out, (void *)r->d_stat, (void *)r->a_pos,
-                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_out})
+                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_pool})
         if (p) cudaFree(p);
+    fd2_destroy(r->audit);
     for (cudaEvent_t e : r->ev)
         if (e) cudaEventDestroy(e);
     delete r;
@@ -99,6 +109,7 @@ struct RouteArgs {
     uint32_t *ev_nchunks;
     NormParams norm;
     fd2_sg_hull hull;
+    float lateral;  // largest |x - centre|, |y - centre| a surrogate row may have
     float audit_frac;
     uint32_t k0, k1;
     int64_t event_base;
@@ -123,7 +134,7 @@ __global__ void route_kernel(const RouteArgs a)
         f[5] = g.beta;
         f[6] = 1.0f - g.top_absfrac;
         f[7] = g.mu > 0.0f ? log10f(g.mu) : -INFINITY;
-        bool in = true;
+        bool in = fabsf(p.x - 0.5f * g.xdet) <= a.lateral && fabsf(p.y - 0.5f * g.ydet) <= a.lateral;
 #pragma unroll
         for (int i = 0; i < kFeatures; ++i) in = in && f[i] >= a.hull.lo[i] && f[i] <= a.hull.hi[i];
         if (!in) {
@@ -165,6 +176,32 @@ struct SampleArgs {
     const uint32_t *run_tag;
 };
 
+constexpr uint32_t kDomainRetry = 0x52455452u;  // rejection retries of ring_radius
+constexpr uint32_t kDomainTurn = 0x5455524eu;   // azimuth retries
+
+// Radius from one ring component, density proportional to r N(r; mu, sd) on
+// r >= 0, exactly.  In t = (r - mu) / sd the weight (mu + sd t) phi(t) splits
+// into t >= 0: mu phi(t) (mass mu / 2, a half-normal) and sd t phi(t) (mass
+// sd phi(0), a Rayleigh), and t0 <= t < 0, t0 = -mu / sd: a normal on
+// [t0, 0) thinned with acceptance 1 + sd t / mu (mass S - mu / 2 - sd phi(0),
+// at least half of its proposals accepted).  u picks the region, v is the
+// region's uniform; rejections draw fresh uniforms.
+__device__ __forceinline__ float ring_radius(float mu, float sd, float S, float u, float v, uint32_t i, uint64_t ge,
+                                             uint32_t run, uint32_t k0, uint32_t k1)
+{
+    const float m1 = 0.5f * mu, m2 = sd * 0.3989422804014327f;
+    const float x = u * S;
+    if (x < m1) return mu + sd * normcdfinvf(0.5f + 0.5f * fminf(v, 1.0f - 6e-8f));
+    if (x < m1 + m2 || mu <= 0.0f) return mu + sd * sqrtf(-2.0f * logf(v));
+    const float t0 = -mu / sd, c0 = normcdff(t0), span = 0.5f - c0;
+    for (uint32_t k = 0; k < 64; ++k) {
+        const uint4 h = philox10(make_uint4(i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainRetry, run * 64u + k), k0, k1);
+        const float t = fminf(normcdfinvf(fmaxf(c0 + unit(h.x) * span, 1e-37f)), 0.0f);
+        if (unit(h.y) <= 1.0f + sd * t / mu) return fmaxf(mu + sd * t, 0.0f);
+    }
+    return 0.5f * mu;  // not reached in practice (acceptance >= 1/2 per proposal)
+}
+
 // Detected photons of one row and their PRF pixels; one warp per row.
 __global__ void sample_kernel(const SampleArgs a)
 {
@@ -184,13 +221,13 @@ __global__ void sample_kernel(const SampleArgs a)
         const float z = o[0];
         const float p = 1.0f / (1.0f + expf(-z));
         const int32_t lo = (int32_t)(((int64_t)N * lane) >> 5), hi = (int32_t)(((int64_t)N * (lane + 1)) >> 5);
-        const int32_t m = hi - lo;
+        const int32_t span = hi - lo;
         int32_t k = 0;
-        if (m > 0 && p > 0.0f) {
+        if (span > 0 && p > 0.0f) {
             if (p >= 1.0f) {
-                k = m;
+                k = span;
             } else {
-                // count the rarer outcome by geometric skips: expected m min(p, 1 - p) + 1 draws
+                // count the rarer outcome by geometric skips: expected span min(p, 1 - p) + 1 draws
                 const bool flip = p > 0.5f;
                 const float q = flip ? 1.0f - p : p;
                 const float inv_log = 1.0f / log1pf(-q);
@@ -206,7 +243,7 @@ __global__ void sample_kernel(const SampleArgs a)
                     for (int j = 0; j < 4; ++j) {
                         const float skip = floorf(logf(unit(w4[j])) * inv_log);
                         const float next = (float)at + skip + 1.0f;
-                        if (next >= (float)m) {
+                        if (next >= (float)span) {
                             done = true;
                             break;
                         }
@@ -215,7 +252,7 @@ __global__ void sample_kernel(const SampleArgs a)
                     }
                     if (done) break;
                 }
-                k = flip ? m - hits : hits;
+                k = flip ? span - hits : hits;
             }
         }
         // warp total and this lane's first detected index
@@ -226,38 +263,40 @@ __global__ void sample_kernel(const SampleArgs a)
             if (lane >= d) before += v;
         }
         const int32_t total = __shfl_sync(0xffffffffu, before, 31);
-        // ---- positions of the detected photons from the truncated mixture
-        float w[kComponents], mu[kComponents], sd[kComponents], c0[kComponents], S[kComponents];
+        // ---- positions of the detected photons: a ring component by weight,
+        // its radius drawn exactly (ring_radius), an azimuth uniform over the
+        // directions that keep the photon on the detector
+        Mix m;
+        decode_mix(o, m);
+        float cumw[kComponents];
         {
-            float amax = o[1];
-            for (int c = 1; c < kComponents; ++c) amax = fmaxf(amax, o[1 + c]);
-            float tot = 0.0f;
-            for (int c = 0; c < kComponents; ++c) {
-                mu[c] = kMuScale * o[1 + kComponents + c];
-                sd[c] = kSdScale * expf(fminf(fmaxf(o[1 + 2 * kComponents + c], kLogSdMin), kLogSdMax));
-                c0[c] = normcdff(-mu[c] / sd[c]);
-                S[c] = 1.0f - c0[c];
-                w[c] = expf(o[1 + c] - amax) * S[c];
-                tot += w[c];
-            }
             float acc = 0.0f;
+#pragma unroll
             for (int c = 0; c < kComponents; ++c) {
-                acc += w[c] / tot;
-                w[c] = acc;  // cumulative
+                acc += m.w[c];
+                cumw[c] = acc;
             }
-            w[kComponents - 1] = 2.0f;
+            cumw[kComponents - 1] = 2.0f;
         }
         int32_t in_prf = 0;
         for (int32_t i = lane; i < total; i += 32) {
             const uint4 h = philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainPlace, run),
                                      a.k0, a.k1);
-            const float u1 = unit(h.x);
+            const float u = unit(h.x);
             int c = 0;
-            while (c < kComponents - 1 && u1 >= w[c]) ++c;
-            const float qv = fminf(fmaxf(c0[c] + unit(h.y) * S[c], 1e-7f), 1.0f - 6e-8f);
-            const float rad = fmaxf(mu[c] + sd[c] * normcdfinvf(qv), 0.0f);
+            while (c < kComponents - 1 && u >= cumw[c]) ++c;
+            const float rad = ring_radius(m.mu[c], m.sd[c], m.S[c], unit(h.y), unit(h.w), (uint32_t)i, ge, run,
+                                          a.k0, a.k1);
             float sn, cs;
             sincospif(2.0f * unit(h.z), &sn, &cs);
+            for (uint32_t k = 0; k < 32; ++k) {
+                const float tx = pos.x + rad * cs, ty = pos.y + rad * sn;
+                if (tx >= 0.0f && tx <= g.xdet && ty >= 0.0f && ty <= g.ydet) break;
+                const uint4 hk =
+                    philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainTurn, run * 32u + k),
+                             a.k0, a.k1);
+                sincospif(2.0f * unit(hk.x), &sn, &cs);
+            }
             const float x = pos.x + rad * cs, y = pos.y + rad * sn;
             if (x <= g.ub_x && y <= g.ub_y && x >= g.lb_x && y >= g.lb_y) {
                 const int ii = (int)floorf(__fdiv_rn(x - g.lb_x, g.pixel));
@@ -283,20 +322,31 @@ __global__ void sample_kernel(const SampleArgs a)
     }
 }
 
-// Compact copies of the audited rows.
+// Compact copies of the audited rows (position, photons, geometry) and
+// their pooled predictions: sum N p q_j over the radial categories j, sum N p,
+// sum N p (1 - p) and sum N (FP64 atomics; one thread per row).
 __global__ void audit_gather_kernel(const int *count, const int32_t *audit_row, const int32_t *sg_event,
                                     const int32_t *sg_n, const float *out, const float4 *ev_pos,
-                                    const uint16_t *ev_geom, float4 *a_pos, int32_t *a_n, int32_t *a_geom,
-                                    float *a_out)
+                                    const uint16_t *ev_geom, int bins, float r_max, float4 *a_pos, int32_t *a_n,
+                                    int32_t *a_geom, double *pool)
 {
     const int n = count[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int r = audit_row[i];
         const int32_t e = sg_event[r];
+        const int32_t N = sg_n[r];
         a_pos[i] = ev_pos[e];
-        a_n[i] = sg_n[r];
+        a_n[i] = N;
         a_geom[i] = ev_geom ? ev_geom[e] : 0;
-        for (int k = 0; k < kOutputs; ++k) a_out[(int64_t)i * kOutputs + k] = out[(int64_t)r * kOutPad + k];
+        const float *o = out + (int64_t)r * kOutPad;
+        const float p = 1.0f / (1.0f + expf(-o[0]));
+        Mix m;
+        decode_mix(o, m);
+        const double np = (double)N * p;
+        for (int j = 0; j <= bins; ++j) atomicAdd(&pool[j], np * (double)bin_prob(m, j, bins, r_max));
+        atomicAdd(&pool[bins + 1], np);
+        atomicAdd(&pool[bins + 2], np * (1.0 - (double)p));
+        atomicAdd(&pool[bins + 3], (double)N);
     }
 }
 
@@ -325,38 +375,6 @@ fd2_status ensure_run_buffers(fd2_sg *s, int64_t n)
         return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "run buffers for " + std::to_string(n) + " events");
     r->cap = n;
     return FD2_OK;
-}
-
-double phi_cdf(double x) { return 0.5 * std::erfc(-x / std::sqrt(2.0)); }
-
-// Bin probabilities of one row's truncated mixture (bins + 1 categories).
-void bin_probs(const float *o, int bins, double width, double *q)
-{
-    double w[kComponents], mu[kComponents], sd[kComponents];
-    double amax = o[1];
-    for (int k = 1; k < kComponents; ++k) amax = std::max(amax, (double)o[1 + k]);
-    double ws = 0.0;
-    for (int k = 0; k < kComponents; ++k) {
-        w[k] = std::exp(o[1 + k] - amax);
-        ws += w[k];
-        mu[k] = kMuScale * o[1 + kComponents + k];
-        sd[k] = kSdScale * std::exp(std::min(std::max((double)o[1 + 2 * kComponents + k], (double)kLogSdMin),
-                                             (double)kLogSdMax));
-    }
-    double Z = 0.0;
-    for (int k = 0; k < kComponents; ++k) Z += w[k] / ws * phi_cdf(mu[k] / sd[k]);
-    for (int j = 0; j <= bins; ++j) {
-        double A = 0.0;
-        for (int k = 0; k < kComponents; ++k) {
-            const double alo = (j * width - mu[k]) / sd[k];
-            const double ahi = j < bins ? ((j + 1) * width - mu[k]) / sd[k] : INFINITY;
-            // lower-tail differences left of the mean, upper-tail ones right of it
-            const double P = alo >= 0.0 ? phi_cdf(-alo) - (j < bins ? phi_cdf(-ahi) : 0.0)
-                                        : (j < bins ? phi_cdf(ahi) : 1.0) - phi_cdf(alo);
-            A += w[k] / ws * std::max(P, 0.0);
-        }
-        q[j] = Z > 0 ? A / Z : 0.0;
-    }
 }
 
 }  // namespace
@@ -403,6 +421,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
             a.hull.lo[i] -= tol;
             a.hull.hi[i] += tol;
         }
+        a.lateral = s->lateral_um;
         a.audit_frac = (float)audit_fraction;
         a.k0 = k0;
         a.k1 = k1;
@@ -480,40 +499,66 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
     const int na = counts[1];
     if (na > 0) {
         RunBuffers *B = R;
+        const int nb = s->bins + 1;
         if (na > B->a_cap) {
-            if (alloc(&B->a_pos, (size_t)na) || alloc(&B->a_n, (size_t)na) || alloc(&B->a_geom, (size_t)na) ||
-                alloc(&B->a_out, (size_t)na * kOutputs))
+            if (alloc(&B->a_pos, (size_t)na) || alloc(&B->a_n, (size_t)na) || alloc(&B->a_geom, (size_t)na))
                 return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "audit buffers");
             B->a_cap = na;
         }
-        audit_gather_kernel<<<(unsigned)std::min((na + 255) / 256, 4096), 256, 0, q>>>(
-            R->d_count, R->audit_row, R->sg_event, R->sg_n, R->out, c->d_ev_pos, c->has_geom ? c->d_ev_geom : nullptr,
-            B->a_pos, B->a_n, B->a_geom, B->a_out);
+        if (!B->a_pool && alloc(&B->a_pool, (size_t)nb + 3))
+            return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "audit buffers");
+        e = cudaMemsetAsync(B->a_pool, 0, sizeof(double) * (nb + 3), q);
+        if (e == cudaSuccess) {
+            audit_gather_kernel<<<(unsigned)std::min((na + 127) / 128, 4096), 128, 0, q>>>(
+                R->d_count, R->audit_row, R->sg_event, R->sg_n, R->out, c->d_ev_pos,
+                c->has_geom ? c->d_ev_geom : nullptr, s->bins, (float)s->radial_max, B->a_pos, B->a_n, B->a_geom,
+                B->a_pool);
+            e = cudaGetLastError();
+        }
         std::vector<float4> pos((size_t)na);
         std::vector<int32_t> nph((size_t)na), geo((size_t)na);
-        std::vector<float> ao((size_t)na * kOutputs);
-        e = cudaGetLastError();
+        std::vector<double> pool((size_t)nb + 3);
         if (e == cudaSuccess) e = cudaMemcpyAsync(pos.data(), B->a_pos, sizeof(float4) * na, cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess) e = cudaMemcpyAsync(nph.data(), B->a_n, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess) e = cudaMemcpyAsync(geo.data(), B->a_geom, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(ao.data(), B->a_out, sizeof(float) * na * kOutputs, cudaMemcpyDeviceToHost, q);
+            e = cudaMemcpyAsync(pool.data(), B->a_pool, sizeof(double) * (nb + 3), cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess) e = cudaStreamSynchronize(q);
         if (e != cudaSuccess) return sg_cuda(s, e, "audit gather");
-        // the audited depositions through the Monte Carlo, label mode
-        fd2_params ap = c->params;
-        ap.num_hist = na;
-        fd2_options ao_opt = c->opt;
-        ao_opt.count_mode = FD2_COUNT_GIVEN;
-        ao_opt.seed = c->opt.seed ^ 0xA0D17A0D17ull;
-        ao_opt.radial_bins = s->bins;
-        ao_opt.radial_max_um = s->radial_max;
-        ao_opt.event_base = 0;
-        ao_opt.tune_cache = nullptr;
-        ao_opt.wait_timeout_s = 0.0;
-        fd2_ctx *ac = nullptr;
-        st = fd2_create(&ap, &ao_opt, &ac);
-        if (st == FD2_OK && c->geoms.size() > 1) st = fd2_set_geometries(ac, c->geoms.data(), (int32_t)c->geoms.size());
+        // the audited depositions through the Monte Carlo in label mode, in a
+        // context kept across runs (re-made when the geometries change or the
+        // audit outgrows it)
+        const bool same = B->audit && B->audit_geoms.size() == c->geoms.size() &&
+                          std::memcmp(B->audit_geoms.data(), c->geoms.data(),
+                                      sizeof(fd2_geometry) * c->geoms.size()) == 0 &&
+                          std::memcmp(&B->audit_params, &c->params, sizeof(fd2_params)) == 0;
+        st = FD2_OK;
+        if (!same || na > B->audit_cap) {
+            fd2_destroy(B->audit);
+            B->audit = nullptr;
+            fd2_params ap = c->params;
+            ap.num_hist = std::max(na, B->audit_cap * 2);
+            fd2_options ao = c->opt;
+            ao.count_mode = FD2_COUNT_GIVEN;
+            ao.seed = c->opt.seed ^ 0xA0D17A0D17ull;
+            ao.radial_bins = s->bins;
+            ao.radial_max_um = s->radial_max;
+            ao.event_base = 0;
+            ao.tune_cache = nullptr;
+            ao.wait_timeout_s = 0.0;
+            st = fd2_create(&ap, &ao, &B->audit);
+            if (st == FD2_OK && c->geoms.size() > 1)
+                st = fd2_set_geometries(B->audit, c->geoms.data(), (int32_t)c->geoms.size());
+            if (st != FD2_OK) {
+                fd2_destroy(B->audit);
+                B->audit = nullptr;
+                return sg_fail(s, st, "audit context");
+            }
+            B->audit_cap = ap.num_hist;
+            B->audit_geoms = c->geoms;
+            B->audit_params = c->params;
+        }
+        fd2_ctx *ac = B->audit;
         std::vector<float> xs((size_t)na), ys((size_t)na), zs((size_t)na);
         std::vector<int32_t> hist((size_t)na);
         std::vector<uint16_t> gg((size_t)na);
@@ -524,43 +569,26 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
             hist[(size_t)i] = i + 1;
             gg[(size_t)i] = (uint16_t)geo[(size_t)i];
         }
+        st = fd2_reset_tallies(ac);
         if (st == FD2_OK)
             st = fd2_submit_events_um(ac, xs.data(), ys.data(), zs.data(), nullptr, hist.data(), nph.data(),
                                       c->geoms.size() > 1 ? gg.data() : nullptr, na);
         if (st == FD2_OK) st = fd2_run(ac);
         if (st == FD2_OK) st = fd2_wait(ac);
-        std::vector<int32_t> det((size_t)na);
-        const int nb = s->bins + 1;
-        std::vector<uint32_t> rad((size_t)na * nb);
-        if (st == FD2_OK) st = fd2_get_detected_per_primary(ac, det.data(), na);
+        std::vector<uint32_t> rad((size_t)B->audit_cap * nb);
         if (st == FD2_OK) st = fd2_get_radial(ac, rad.data(), (int64_t)rad.size());
-        const std::string aerr = ac ? fd2_last_error(ac) : "";
-        fd2_destroy(ac);
-        if (st != FD2_OK) return sg_fail(s, st, "audit Monte Carlo: " + aerr);
-        double mc = 0, expct = 0, var = 0, ph = 0;
-        std::vector<double> hmc((size_t)nb, 0.0), hsg((size_t)nb, 0.0), qv((size_t)nb);
-        const double width = s->radial_max / s->bins;
-        for (int i = 0; i < na; ++i) {
-            const float *o = &ao[(size_t)i * kOutputs];
-            const double p = 1.0 / (1.0 + std::exp(-(double)o[0]));
-            const double N = nph[(size_t)i];
-            mc += det[(size_t)i];
-            expct += N * p;
-            var += N * p * (1.0 - p);
-            ph += N;
-            bin_probs(o, s->bins, width, qv.data());
-            for (int j = 0; j < nb; ++j) {
-                hmc[(size_t)j] += rad[(size_t)i * nb + j];
-                hsg[(size_t)j] += N * p * qv[(size_t)j];
-            }
-        }
-        double smc = 0, ssg = 0, l1 = 0;
-        for (int j = 0; j < nb; ++j) {
-            smc += hmc[(size_t)j];
-            ssg += hsg[(size_t)j];
-        }
+        if (st != FD2_OK) return sg_fail(s, st, std::string("audit Monte Carlo: ") + fd2_last_error(ac));
+        // every detected photon is in exactly one radial category
+        std::vector<double> hmc((size_t)nb, 0.0);
+        double mc = 0.0;
+        for (int i = 0; i < na; ++i)
+            for (int j = 0; j < nb; ++j) hmc[(size_t)j] += rad[(size_t)i * nb + j];
+        for (int j = 0; j < nb; ++j) mc += hmc[(size_t)j];
+        const double expct = pool[(size_t)nb], var = pool[(size_t)nb + 1], ph = pool[(size_t)nb + 2];
+        double ssg = 0.0, l1 = 0.0;
+        for (int j = 0; j < nb; ++j) ssg += pool[(size_t)j];
         for (int j = 0; j < nb; ++j)
-            l1 += std::fabs((smc > 0 ? hmc[(size_t)j] / smc : 0) - (ssg > 0 ? hsg[(size_t)j] / ssg : 0));
+            l1 += std::fabs((mc > 0 ? hmc[(size_t)j] / mc : 0) - (ssg > 0 ? pool[(size_t)j] / ssg : 0));
         out.audit_mc_detected = mc;
         out.audit_sg_expected = expct;
         out.audit_photons = ph;

@@ -10,12 +10,12 @@
 // graph replayed `steps` times; the step counter lives on the device.
 //
 // Loss per point with N photons, d detected and radial label counts h_j
-// (j < R inside radial_max_um, j = R beyond):
+// (j < R: quadratic bins inside radial_max_um, j = R beyond):
 //   L = BCE(sigmoid(out0), d / N)
 //     + lambda * sum_j y_j (-log q_j),   y_j = h_j / sum h
-// with q_j the probability of bin j under the mixture
-//   sum_k w_k N(r; mu_k, s_k) restricted to r >= 0,
-//   w = softmax(out[1..8]), mu = 50 um * out[9..16],
+// with q_j the probability of bin j under the mixture of Gaussian rings
+//   PRF(r) = sum_k w_k N(r; mu_k, s_k) / S_k per unit area (fd2_sg_mix.cuh),
+//   w = softmax(out[1..8]), mu = 50 um * softplus(out[9..16]),
 //   s = 10 um * exp(clamp(out[17..24], -6, 4)).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -30,6 +30,7 @@
 #include "fd2.h"
 #include "fd2_sg_gemm.cuh"
 #include "fd2_sg_internal.h"
+#include "fd2_sg_mix.cuh"
 #include "fd2_surrogate.h"
 
 using fd2::sg::GemmArgs;
@@ -52,38 +53,11 @@ __device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1)
     return c;
 }
 
-__device__ __forceinline__ float norm_pdf(float a) { return 0.3989422804014327f * expf(-0.5f * a * a); }
-
-// Mixture parameters of one output row.
-struct Mix {
-    float w[kComponents], mu[kComponents], sd[kComponents];
-    bool clamped[kComponents];
-};
-
-__device__ __forceinline__ void decode_mix(const float *o, Mix &m)
-{
-    float amax = o[1];
-#pragma unroll
-    for (int k = 1; k < kComponents; ++k) amax = fmaxf(amax, o[1 + k]);
-    float s = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kComponents; ++k) {
-        m.w[k] = expf(o[1 + k] - amax);
-        s += m.w[k];
-    }
-#pragma unroll
-    for (int k = 0; k < kComponents; ++k) {
-        m.w[k] /= s;
-        m.mu[k] = kMuScale * o[1 + kComponents + k];
-        const float ls = o[1 + 2 * kComponents + k];
-        m.clamped[k] = ls < kLogSdMin || ls > kLogSdMax;
-        m.sd[k] = kSdScale * expf(fminf(fmaxf(ls, kLogSdMin), kLogSdMax));
-    }
-}
-
 // Loss of one point and (optionally) d loss / d out.  y: normalised radial
-// label over nb = bins + 1 categories (null = no radial term).
-__device__ float point_loss(const float *o, float t, const float *y, int bins, float width, float lambda,
+// label over bins + 1 categories (null = no radial term).  The radial term
+// is the cross-entropy -sum_j y_j log q_j of the ring mixture's category
+// probabilities q_j = sum_k w_k M_k(e_j, e_j+1) / S_k (fd2_sg_mix.cuh).
+__device__ float point_loss(const float *o, float t, const float *y, int bins, float r_max, float lambda,
                             float *dout, float *det_loss, float *rad_loss)
 {
     // detection
@@ -103,85 +77,60 @@ __device__ float point_loss(const float *o, float t, const float *y, int bins, f
     }
     Mix m;
     decode_mix(o, m);
-    // Z = sum_k w_k S_k with S_k = 1 - Phi(-mu_k / sd_k)
-    float S[kComponents], a0[kComponents];
-    float Z = 0.0f;
+    // per component: A1 = sum_j c_j M_kj, Amu = sum_j c_j dM_kj/dmu, Asd = sum_j c_j dM_kj/dsd
+    float A1[kComponents], Amu[kComponents], Asd[kComponents];
+    Edge lo[kComponents];
 #pragma unroll
     for (int k = 0; k < kComponents; ++k) {
-        a0[k] = -m.mu[k] / m.sd[k];
-        S[k] = normcdff(-a0[k]);
-        Z += m.w[k] * S[k];
+        A1[k] = 0.0f;
+        Amu[k] = 0.0f;
+        Asd[k] = 0.0f;
+        lo[k] = edge_at(0.0f, false, m.mu[k], m.sd[k]);
     }
-    Z = fmaxf(Z, 1e-30f);
-    float gw[kComponents], gmu[kComponents], gsd[kComponents];
-#pragma unroll
-    for (int k = 0; k < kComponents; ++k) {
-        gw[k] = S[k] / Z;
-        gmu[k] = m.w[k] / Z * norm_pdf(a0[k]) / m.sd[k];
-        gsd[k] = m.w[k] / Z * a0[k] * norm_pdf(a0[k]) / m.sd[k];
-    }
-    float lr = logf(Z);
-    // bins: edges e_j = j * width; the last category is [bins * width, inf).
-    // A bin's mass is a difference of lower-tail CDFs left of the mean and of
-    // upper-tail CDFs right of it, so tail bins keep their relative accuracy.
-    float cdf_lo[kComponents], ccdf_lo[kComponents], pdf_lo[kComponents], alo[kComponents];
-#pragma unroll
-    for (int k = 0; k < kComponents; ++k) {
-        alo[k] = a0[k];
-        cdf_lo[k] = normcdff(alo[k]);
-        ccdf_lo[k] = normcdff(-alo[k]);
-        pdf_lo[k] = norm_pdf(alo[k]);
-    }
+    float lr = 0.0f;
     for (int j = 0; j <= bins; ++j) {
-        const float yj = y[j];
-        float cdf_hi[kComponents], ccdf_hi[kComponents], pdf_hi[kComponents], ahi[kComponents], P[kComponents];
-        float A = 0.0f;
+        const bool top = j >= bins;
+        const float e_hi = top ? 0.0f : radial_edge(j + 1, bins, r_max);
+        float M[kComponents], dM_mu[kComponents], dM_sd[kComponents];
+        Edge hi[kComponents];
+        float q = 0.0f;
 #pragma unroll
         for (int k = 0; k < kComponents; ++k) {
-            if (j < bins) {
-                ahi[k] = ((float)(j + 1) * width - m.mu[k]) / m.sd[k];
-                cdf_hi[k] = normcdff(ahi[k]);
-                ccdf_hi[k] = normcdff(-ahi[k]);
-                pdf_hi[k] = norm_pdf(ahi[k]);
-            } else {
-                ahi[k] = 0.0f;
-                cdf_hi[k] = 1.0f;
-                ccdf_hi[k] = 0.0f;
-                pdf_hi[k] = 0.0f;
-            }
-            P[k] = fmaxf(alo[k] >= 0.0f ? ccdf_lo[k] - ccdf_hi[k] : cdf_hi[k] - cdf_lo[k], 0.0f);
-            A += m.w[k] * P[k];
+            hi[k] = edge_at(e_hi, top, m.mu[k], m.sd[k]);
+            M[k] = ring_mass(lo[k], hi[k], m.mu[k], m.sd[k], &dM_mu[k], &dM_sd[k]);
+            q += m.w[k] * M[k] / m.S[k];
         }
+        const float yj = y[j];
         if (yj > 0.0f) {
-            const float Ae = A + 1e-12f;
-            lr -= yj * logf(Ae);
-            const float c = yj / Ae;
+            const float qe = q + 1e-12f;
+            lr -= yj * logf(qe);
+            const float c = yj / qe;
 #pragma unroll
             for (int k = 0; k < kComponents; ++k) {
-                gw[k] -= c * P[k];
-                // dP/dmu = -(pdf_hi - pdf_lo)/sd ; dP/dsd = -(ahi pdf_hi - alo pdf_lo)/sd
-                gmu[k] -= c * m.w[k] * (-(pdf_hi[k] - pdf_lo[k]) / m.sd[k]);
-                gsd[k] -= c * m.w[k] * (-(ahi[k] * pdf_hi[k] - alo[k] * pdf_lo[k]) / m.sd[k]);
+                A1[k] += c * M[k];
+                Amu[k] += c * dM_mu[k];
+                Asd[k] += c * dM_sd[k];
             }
         }
 #pragma unroll
-        for (int k = 0; k < kComponents; ++k) {
-            cdf_lo[k] = cdf_hi[k];
-            ccdf_lo[k] = ccdf_hi[k];
-            pdf_lo[k] = pdf_hi[k];
-            alo[k] = ahi[k];
-        }
+        for (int k = 0; k < kComponents; ++k) lo[k] = hi[k];
     }
     *rad_loss = lr;
     if (dout) {
-        float wg = 0.0f;
-#pragma unroll
-        for (int k = 0; k < kComponents; ++k) wg += m.w[k] * gw[k];
+        float gw[kComponents], wg = 0.0f;
 #pragma unroll
         for (int k = 0; k < kComponents; ++k) {
+            gw[k] = -A1[k] / m.S[k];
+            wg += m.w[k] * gw[k];
+        }
+#pragma unroll
+        for (int k = 0; k < kComponents; ++k) {
+            const float f = m.w[k] / m.S[k];
+            const float gmu = -f * (Amu[k] - A1[k] * m.dS_mu[k] / m.S[k]);
+            const float gsd = -f * (Asd[k] - A1[k] * m.dS_sd[k] / m.S[k]);
             dout[1 + k] = lambda * m.w[k] * (gw[k] - wg);
-            dout[1 + kComponents + k] = lambda * kMuScale * gmu[k];
-            dout[1 + 2 * kComponents + k] = m.clamped[k] ? 0.0f : lambda * m.sd[k] * gsd[k];
+            dout[1 + kComponents + k] = lambda * m.dmu[k] * gmu;
+            dout[1 + 2 * kComponents + k] = m.clamped[k] ? 0.0f : lambda * m.sd[k] * gsd;
         }
     }
     return ld + lambda * lr;
@@ -232,7 +181,7 @@ __global__ void gather_kernel(const float *__restrict__ feat, const int32_t *__r
 // set, dL/dout / b as BF16 [b][64].
 __global__ void loss_kernel(const float *__restrict__ out, int ldo, const float *__restrict__ target,
                             const float *__restrict__ ylab, const float *__restrict__ has_rad, int bins,
-                            float width, float lambda, int b, float scale, __nv_bfloat16 *__restrict__ dout,
+                            float r_max, float lambda, int b, float scale, __nv_bfloat16 *__restrict__ dout,
                             double *acc)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -241,7 +190,7 @@ __global__ void loss_kernel(const float *__restrict__ out, int ldo, const float 
         float o[kOutputs], g[kOutputs];
         for (int i = 0; i < kOutputs; ++i) o[i] = out[(int64_t)r * ldo + i];
         const bool rad = has_rad[r] > 0.0f;
-        lt = point_loss(o, target[r], rad ? ylab + (int64_t)r * (bins + 1) : nullptr, bins, width, lambda,
+        lt = point_loss(o, target[r], rad ? ylab + (int64_t)r * (bins + 1) : nullptr, bins, r_max, lambda,
                         dout ? g : nullptr, &ld, &lrad);
         if (dout) {
             for (int i = 0; i < kOutputs; ++i) dout[(int64_t)r * kOutPad + i] = __float2bfloat16(g[i] * scale);
@@ -300,10 +249,11 @@ __global__ void split_sum_kernel(const float *__restrict__ ws, int splits, int64
 // Adam on the FP32 masters, then the BF16 copies.  `mask` zeroes the update
 // of padding entries (their gradients are zero anyway).
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
-                            float *__restrict__ v, __nv_bfloat16 *__restrict__ pb, int64_t n, float lr, float b1,
+                            float *__restrict__ v, __nv_bfloat16 *__restrict__ pb, int64_t n, const float *lr_ptr, float b1,
                             float b2, float eps, unsigned long long *step, const uint8_t *__restrict__ live)
 {
     const unsigned long long t = *step + 1;
+    const float lr = *lr_ptr;
     const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         if (!live[i]) continue;
@@ -488,10 +438,10 @@ cudaError_t train_step(fd2_sg *s, cudaStream_t st)
                                                     s->target, s->ylab, s->has_rad);
     if ((e = sg_forward(s, st, s->x0, B, nullptr, s->h1, s->h2, s->h3, s->out)) != cudaSuccess) return e;
     loss_kernel<<<grid_for(B, 128), 128, 0, st>>>(s->out, kOutPad, s->target, s->ylab, s->has_rad, bins,
-                                                  (float)(s->radial_max / bins), s->lambda, B, 1.0f / (float)B,
+                                                  (float)s->radial_max, s->lambda, B, 1.0f / (float)B,
                                                   s->dout, s->d_acc);
     if ((e = backward(s, st, B)) != cudaSuccess) return e;
-    adam_kernel<<<grid_for(s->n_params, 256), 256, 0, st>>>(s->p, s->g, s->m, s->v, s->pb, s->n_params, s->lr,
+    adam_kernel<<<grid_for(s->n_params, 256), 256, 0, st>>>(s->p, s->g, s->m, s->v, s->pb, s->n_params, s->d_lr,
                                                             s->beta1, s->beta2, s->eps, s->d_step, s->d_live);
     step_kernel<<<1, 1, 0, st>>>(s->d_step);
     return cudaGetLastError();
@@ -579,8 +529,8 @@ fd2_status upload_params(fd2_sg *s, const std::vector<float> &master)
 void set_norm(fd2_sg *s)
 {
     for (int i = 0; i < kFeatures; ++i) {
-        s->norm.lo[i] = s->hull.lo[i];
-        const float span = s->hull.hi[i] - s->hull.lo[i];
+        s->norm.lo[i] = s->norm_box.lo[i];
+        const float span = s->norm_box.hi[i] - s->norm_box.lo[i];
         s->norm.inv[i] = span > 0.0f ? 1.0f / span : 0.5f;  // constant feature -> 0 after 2(f-lo)*inv - 1 + 1
     }
 }
@@ -626,14 +576,15 @@ void fd2_sg_default_config(fd2_sg_config *c)
     std::memset(c, 0, sizeof *c);
     c->device = 0;
     c->hidden = 256;
-    c->radial_bins = 64;
-    c->radial_max_um = 200.0;
+    c->radial_bins = 96;
+    c->radial_max_um = 400.0;
     c->batch = 8192;
     c->lr = 1e-3f;
     c->beta1 = 0.9f;
     c->beta2 = 0.999f;
     c->adam_eps = 1e-8f;
     c->radial_weight = 1.0f;
+    c->lateral_um = 50.0f;
     c->seed = 0x5347fd2ull;
 }
 
@@ -647,7 +598,8 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     if (cfg) c = *cfg;
     else fd2_sg_default_config(&c);
     if (c.hidden < 64 || c.hidden % 64 || c.hidden > 1024 || c.radial_bins < 1 || c.radial_bins > 1024 ||
-        !(c.radial_max_um > 0) || c.batch < 64 || c.batch % 64 || c.batch > (1 << 20) || !(c.lr > 0))
+        !(c.radial_max_um > 0) || c.batch < 64 || c.batch % 64 || c.batch > (1 << 20) || !(c.lr > 0) ||
+        !(c.lateral_um >= 0))
         return FD2_ERR_INVALID_ARGUMENT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return FD2_ERR_NO_DEVICE;
@@ -663,10 +615,13 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     s->beta2 = c.beta2;
     s->eps = c.adam_eps;
     s->lambda = c.radial_weight;
+    s->lateral_um = c.lateral_um;
     s->seed = c.seed;
     for (int i = 0; i < kFeatures; ++i) {
         s->hull.lo[i] = 0.0f;
         s->hull.hi[i] = 1.0f;
+        s->norm_box.lo[i] = 0.0f;
+        s->norm_box.hi[i] = 1.0f;
     }
     set_norm(s);
     auto bail = [&](fd2_status st) {
@@ -678,9 +633,10 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     layout(s);
     const size_t P = (size_t)s->n_params;
     if (alloc(&s->p, P) || alloc(&s->g, P) || alloc(&s->m, P) || alloc(&s->v, P) || alloc(&s->pb, P) ||
-        alloc(&s->d_live, P) || alloc(&s->d_step, 1) || alloc(&s->d_acc, 4) ||
+        alloc(&s->d_live, P) || alloc(&s->d_step, 1) || alloc(&s->d_acc, 4) || alloc(&s->d_lr, 1) ||
         alloc(&s->ws, (size_t)kMaxSplits * std::max<size_t>((size_t)s->hidden * s->hidden, (size_t)kOutPad * s->hidden)))
         return bail(FD2_ERR_OUT_OF_MEMORY);
+    if (cudaMemcpy(s->d_lr, &s->lr, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return bail(FD2_ERR_CUDA);
     const std::vector<uint8_t> live = live_mask(s);
     if (cudaMemcpy(s->d_live, live.data(), P, cudaMemcpyHostToDevice) != cudaSuccess) return bail(FD2_ERR_CUDA);
     if (cudaMemset(s->g, 0, sizeof(float) * P) != cudaSuccess) return bail(FD2_ERR_CUDA);
@@ -709,7 +665,8 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     for (int r = 0; r < kOutputs; ++r)
         for (int64_t cc = 0; cc < H; ++cc) master[(size_t)(s->off[kW4] + r * H + cc)] = (float)(gauss() * 0.01);
     for (int k = 0; k < kComponents; ++k) {
-        master[(size_t)(s->off[kB4] + 1 + kComponents + k)] = 0.05f + 0.15f * k;               // mu: 2.5 .. 55 um
+        const double mu0 = (2.5 + 7.5 * k) / kMuScale;                                          // 2.5 .. 55 um
+        master[(size_t)(s->off[kB4] + 1 + kComponents + k)] = (float)std::log(std::expm1(mu0));  // softplus^-1
         master[(size_t)(s->off[kB4] + 1 + 2 * kComponents + k)] = std::log(0.2f + 0.4f * k);  // sd: 2 .. 30 um
     }
     fd2_status r = upload_params(s, master);
@@ -725,7 +682,7 @@ void fd2_sg_destroy(fd2_sg *s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     for (void *p : {(void *)s->p, (void *)s->g, (void *)s->m, (void *)s->v, (void *)s->pb, (void *)s->d_live,
-                    (void *)s->d_step, (void *)s->d_acc, (void *)s->ws, (void *)s->x0, (void *)s->h1, (void *)s->h2,
+                    (void *)s->d_step, (void *)s->d_acc, (void *)s->d_lr, (void *)s->ws, (void *)s->x0, (void *)s->h1, (void *)s->h2,
                     (void *)s->h3, (void *)s->d1, (void *)s->d2, (void *)s->d3, (void *)s->out, (void *)s->dout,
                     (void *)s->target, (void *)s->has_rad, (void *)s->ylab, (void *)s->d_feat, (void *)s->d_photons,
                     (void *)s->d_detected, (void *)s->d_radial})
@@ -736,6 +693,16 @@ void fd2_sg_destroy(fd2_sg *s)
 }
 
 int64_t fd2_sg_num_params(const fd2_sg *s) { return s ? public_count(s) : 0; }
+
+fd2_status fd2_sg_set_lr(fd2_sg *s, float lr)
+{
+    if (!s || !(lr > 0.0f) || !std::isfinite(lr)) return FD2_ERR_INVALID_ARGUMENT;
+    SG_CUDA(s, cudaSetDevice(s->device));
+    SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->lr = lr;
+    SG_CUDA(s, cudaMemcpy(s->d_lr, &s->lr, sizeof(float), cudaMemcpyHostToDevice));
+    return FD2_OK;
+}
 
 fd2_status fd2_sg_get_params(fd2_sg *s, float *params, int64_t n)
 {
@@ -770,7 +737,13 @@ fd2_status fd2_sg_set_hull(fd2_sg *s, const fd2_sg_hull *h)
         if (!(std::isfinite(h->lo[i]) && std::isfinite(h->hi[i]) && h->hi[i] >= h->lo[i]))
             return FD2_ERR_INVALID_ARGUMENT;
     s->hull = *h;
-    set_norm(s);
+    if (!s->norm_fixed) {
+        // the network's input normalisation comes from its first hull and
+        // stays with the network (later hulls only change the routing)
+        s->norm_box = *h;
+        s->norm_fixed = true;
+        set_norm(s);
+    }
     if (s->graph) cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
     return FD2_OK;
@@ -835,7 +808,7 @@ fd2_status fd2_sg_eval(fd2_sg *s, float *loss, float *det_loss, float *radial_lo
                                                                s->has_rad);
         SG_CUDA(s, sg_forward(s, s->stream, s->x0, b, nullptr, s->h1, s->h2, s->h3, s->out));
         loss_kernel<<<grid_for(b, 128), 128, 0, s->stream>>>(s->out, kOutPad, s->target, s->ylab, s->has_rad,
-                                                             s->bins, (float)(s->radial_max / s->bins), s->lambda, b,
+                                                             s->bins, (float)s->radial_max, s->lambda, b,
                                                              1.0f, nullptr, s->d_acc);
         SG_CUDA(s, cudaGetLastError());
     }
@@ -914,7 +887,7 @@ fd2_status fd2_sg_loss_grad(fd2_sg *s, const float *features, const int32_t *pho
     }
     if (e == cudaSuccess) {
         loss_kernel<<<grid_for(b, 128), 128, 0, s->stream>>>(s->out, kOutPad, s->target, s->ylab, s->has_rad,
-                                                             s->bins, (float)(s->radial_max / s->bins), s->lambda, b,
+                                                             s->bins, (float)s->radial_max, s->lambda, b,
                                                              1.0f / (float)b, s->dout, s->d_acc);
         e = backward(s, s->stream, b);
     }
@@ -963,7 +936,8 @@ fd2_status fd2_sg_predict(fd2_sg *s, const float *features, int64_t n, float *ou
     return FD2_OK;
 }
 
-// File: "FD2SG001", hidden, bins, radial_max, hull, public parameters.
+// File: "FD2SG002", hidden, bins, radial_max, normalisation box, routing
+// hull, public parameters.
 fd2_status fd2_sg_save(fd2_sg *s, const char *path)
 {
     if (!s || !path) return FD2_ERR_INVALID_ARGUMENT;
@@ -973,8 +947,10 @@ fd2_status fd2_sg_save(fd2_sg *s, const char *path)
     FILE *f = std::fopen(path, "wb");
     if (!f) return sg_fail(s, FD2_ERR_IO, std::string("cannot write ") + path);
     const int32_t hdr[2] = {s->hidden, s->bins};
-    bool ok = std::fwrite("FD2SG001", 1, 8, f) == 8 && std::fwrite(hdr, sizeof hdr, 1, f) == 1 &&
-              std::fwrite(&s->radial_max, sizeof(double), 1, f) == 1 && std::fwrite(&s->hull, sizeof s->hull, 1, f) == 1 &&
+    bool ok = std::fwrite("FD2SG002", 1, 8, f) == 8 && std::fwrite(hdr, sizeof hdr, 1, f) == 1 &&
+              std::fwrite(&s->radial_max, sizeof(double), 1, f) == 1 &&
+              std::fwrite(&s->norm_box, sizeof s->norm_box, 1, f) == 1 &&
+              std::fwrite(&s->hull, sizeof s->hull, 1, f) == 1 &&
               std::fwrite(p.data(), sizeof(float), p.size(), f) == p.size();
     ok = (std::fclose(f) == 0) && ok;
     return ok ? FD2_OK : sg_fail(s, FD2_ERR_IO, std::string("write failed: ") + path);
@@ -988,17 +964,20 @@ fd2_status fd2_sg_load(fd2_sg *s, const char *path)
     char magic[8];
     int32_t hdr[2];
     double rmax = 0;
-    fd2_sg_hull h;
+    fd2_sg_hull nb, h;
     std::vector<float> p((size_t)public_count(s));
-    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "FD2SG001", 8) == 0 &&
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "FD2SG002", 8) == 0 &&
               std::fread(hdr, sizeof hdr, 1, f) == 1 && std::fread(&rmax, sizeof rmax, 1, f) == 1 &&
-              std::fread(&h, sizeof h, 1, f) == 1;
+              std::fread(&nb, sizeof nb, 1, f) == 1 && std::fread(&h, sizeof h, 1, f) == 1;
     ok = ok && hdr[0] == s->hidden && hdr[1] == s->bins && rmax == s->radial_max &&
          std::fread(p.data(), sizeof(float), p.size(), f) == p.size();
     std::fclose(f);
     if (!ok) return sg_fail(s, FD2_ERR_IO, std::string("not a matching surrogate file: ") + path);
     fd2_status st = fd2_sg_set_params(s, p.data(), (int64_t)p.size());
     if (st != FD2_OK) return st;
+    s->norm_box = nb;
+    s->norm_fixed = true;
+    set_norm(s);
     return fd2_sg_set_hull(s, &h);
 }
 

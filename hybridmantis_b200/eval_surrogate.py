@@ -35,17 +35,21 @@ def _radial(img, cx, cy, edges):
 
 
 def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 4242, audit: float = 0.01,
-             device: int = 0, repeats: int = 2) -> dict:
+             device: int = 0, repeats: int = 2, noise_floor: bool = False) -> dict:
     es = fd.synth_events(config, xrays, seed)
     out = {"config": config, "xrays": es.params.num_hist, "events": es.n}
     res = {}
     with sgm.Surrogate(device=device) as s:
         s.load(model)
-        for mode in ("mc", "sg"):
-            with fd.OpticalTransport(es.params, device=device, seed=seed + 1) as t:
+        for mode in ("mc", "mc2", "sg"):
+            if mode == "mc2" and not noise_floor:
+                continue
+            # mc2: the Monte Carlo again with other random streams (the
+            # noise floor of the comparison)
+            with fd.OpticalTransport(es.params, device=device, seed=seed + (2 if mode == "mc2" else 1)) as t:
                 t.submit(es)
                 # warm-up run, then timed runs on reset tallies
-                if mode == "mc":
+                if mode != "sg":
                     t.run_sync()
                 else:
                     s.run(t, audit)
@@ -54,7 +58,7 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
                 for _ in range(repeats):
                     t.reset_tallies()
                     t0 = time.perf_counter()
-                    if mode == "mc":
+                    if mode != "sg":
                         t.run_sync()
                     else:
                         stats = s.run(t, audit)
@@ -78,10 +82,19 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
         "swank": [res["mc"]["swank"], res["sg"]["swank"]],
         "swank_diff": res["sg"]["swank"] - res["mc"]["swank"],
         "radial_prf_l1": float(np.abs(rm - rs).sum()),
+        "radial_profile": {"edges_um": edges.tolist(), "mc": rm.tolist(), "sg": rs.tolist()},
         "prf_image_l1": float(np.abs(im / im.sum() - isg / isg.sum()).sum()),
         "detected": [res["mc"]["detected"], res["sg"]["detected"]],
         "sg_stats": res["sg"]["stats"],
     })
+    if noise_floor:
+        # the same two comparisons between two Monte Carlo runs of the same
+        # events with different random streams
+        i2 = res["mc2"]["image"]
+        r2 = _radial(i2, cx, cy, edges)
+        out["mc_vs_mc"] = {"radial_prf_l1": float(np.abs(rm - r2).sum()),
+                           "prf_image_l1": float(np.abs(im / im.sum() - i2 / i2.sum()).sum()),
+                           "phs_mean": res["mc2"]["phs_mean"], "swank": res["mc2"]["swank"]}
     return out
 
 
@@ -92,8 +105,9 @@ def main():
     ap.add_argument("--xrays", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=4242)
     ap.add_argument("--audit", type=float, default=0.01)
+    ap.add_argument("--noise-floor", action="store_true")
     a = ap.parse_args()
-    print(json.dumps(evaluate(a.model, a.config, a.xrays, a.seed, a.audit)))
+    print(json.dumps(evaluate(a.model, a.config, a.xrays, a.seed, a.audit, noise_floor=a.noise_floor)))
 
 
 if __name__ == "__main__":

@@ -63,10 +63,12 @@ def sample_geometries(n: int, seed: int, base: Geometry | None = None) -> list:
     return out
 
 
-def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: int = 0, radial_bins: int = 64,
-                 radial_max_um: float = 200.0, energy_kev=(1.0, 80.0)):
+def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: int = 0, radial_bins: int = 96,
+                 radial_max_um: float = 400.0, energy_kev=(1.0, 80.0)):
     """Monte Carlo labels: for each geometry, `points_per_geom` depositions at
-    the detector centre with depth U(0, H), energy U(energy_kev) and in-column
+    the detector centre with depth H u (half of them) or H u^2 (the other
+    half: denser near the entrance surface, where x-rays deposit most and
+    the PRF is widest), u ~ U(0, 1), energy U(energy_kev) and in-column
     offset U(0, 1), each transported with `photons` photons.  Returns
     (features [n, 8], photons [n], detected [n], radial [n, radial_bins + 1])."""
     rng = np.random.default_rng(seed)
@@ -80,7 +82,9 @@ def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: i
             t.set_geometries(gs)
             gi = np.repeat(np.arange(len(gs)), points_per_geom).astype(np.uint16)
             H = np.array([g.det_height for g in gs])[gi]
-            depth = (H * rng.uniform(0.001, 0.999, n)).astype(np.float32).astype(np.float64)
+            u = rng.uniform(0.001, 0.999, n)
+            u = np.where(rng.random(n) < 0.5, u, np.maximum(u * u, 0.001))
+            depth = (H * u).astype(np.float32).astype(np.float64)
             cx = np.array([g.det_x / 2.0 for g in gs])[gi]
             cy = np.array([g.det_y / 2.0 for g in gs])[gi]
             z = H / 2.0 - depth
@@ -103,45 +107,54 @@ def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: i
     return np.concatenate(feats), np.concatenate(phot), np.concatenate(det), np.concatenate(rad)
 
 
+def radial_edges(bins: int = 96, radial_max_um: float = 400.0) -> np.ndarray:
+    """Edges of the radial label bins: r_max (j / bins)^2, j = 0..bins."""
+    return radial_max_um * (np.arange(bins + 1) / bins) ** 2
+
+
 def mixture(out: np.ndarray):
-    """Decode network outputs [n, 25] into (p_detect [n], w [n, 8], mu [n, 8], sd [n, 8]) in um."""
+    """Decode network outputs [n, 25] into (p_detect [n], w [n, 8], ring radii mu [n, 8], widths sd [n, 8]) in um."""
     out = np.asarray(out, np.float64)
     p = 1.0 / (1.0 + np.exp(-out[:, 0]))
     a = out[:, 1:1 + N_COMPONENTS]
     w = np.exp(a - a.max(1, keepdims=True))
     w /= w.sum(1, keepdims=True)
-    mu = MU_SCALE * out[:, 1 + N_COMPONENTS:1 + 2 * N_COMPONENTS]
+    om = out[:, 1 + N_COMPONENTS:1 + 2 * N_COMPONENTS]
+    mu = MU_SCALE * (np.maximum(om, 0) + np.log1p(np.exp(-np.abs(om))))
     sd = SD_SCALE * np.exp(np.clip(out[:, 1 + 2 * N_COMPONENTS:], -6.0, 4.0))
     return p, w, mu, sd
 
 
-def radial_bin_probs(out: np.ndarray, bins: int = 64, radial_max_um: float = 200.0) -> np.ndarray:
-    """Bin probabilities [n, bins + 1] of the truncated mixture (last: overflow)."""
+def radial_bin_probs(out: np.ndarray, bins: int = 96, radial_max_um: float = 400.0) -> np.ndarray:
+    """Category probabilities [n, bins + 1] of the mixture of Gaussian rings
+    (last: beyond radial_max_um): component k has radial density
+    r N(r; mu_k, sd_k) / S_k, mass mu [Phi(t_b) - Phi(t_a)] + sd [phi(t_a) - phi(t_b)]."""
     from scipy.special import ndtr
     _, w, mu, sd = mixture(out)
-    edges = np.arange(bins + 1) * (radial_max_um / bins)
-    a = (edges[None, None, :] - mu[:, :, None]) / sd[:, :, None]
-    a = np.concatenate([a, np.full(a.shape[:2] + (1,), np.inf)], axis=2)
-    c, cc = ndtr(a), ndtr(-a)
-    S = ndtr(mu / sd)
-    lo = a[:, :, :-1]
-    P = np.maximum(np.where(lo >= 0, cc[:, :, :-1] - cc[:, :, 1:], c[:, :, 1:] - c[:, :, :-1]), 0.0)
-    A = (w[:, :, None] * P).sum(1)
-    Z = (w * S).sum(1, keepdims=True)
-    return A / Z
+    e = np.concatenate([radial_edges(bins, radial_max_um), [np.inf]])
+    t = (e[None, None, :] - mu[:, :, None]) / sd[:, :, None]
+    c, cc = ndtr(t), ndtr(-t)
+    ph = np.where(np.isinf(t), 0.0, np.exp(-0.5 * np.where(np.isinf(t), 0.0, t) ** 2) / np.sqrt(2 * np.pi))
+    lo = t[:, :, :-1]
+    dphi = np.maximum(np.where(lo >= 0, cc[:, :, :-1] - cc[:, :, 1:], c[:, :, 1:] - c[:, :, :-1]), 0.0)
+    M = np.maximum(mu[:, :, None] * dphi + sd[:, :, None] * (ph[:, :, :-1] - ph[:, :, 1:]), 0.0)
+    t0 = -mu / sd
+    S = mu * ndtr(-t0) + sd * np.exp(-0.5 * t0 ** 2) / np.sqrt(2 * np.pi)
+    return (w[:, :, None] * M / S[:, :, None]).sum(1)
 
 
 class Surrogate:
     """One surrogate network with its optimizer state on a GPU."""
 
-    def __init__(self, device: int = 0, hidden: int = 256, radial_bins: int = 64, radial_max_um: float = 200.0,
-                 batch: int = 8192, lr: float = 1e-3, radial_weight: float = 1.0, seed: int = 0x5347fd2):
+    def __init__(self, device: int = 0, hidden: int = 256, radial_bins: int = 96, radial_max_um: float = 400.0,
+                 batch: int = 8192, lr: float = 1e-3, radial_weight: float = 1.0, seed: int = 0x5347fd2,
+                 lateral_um: float = 50.0):
         lib = load()
         self._lib = lib
         c = SgConfig()
         lib.fd2_sg_default_config(ctypes.byref(c))
         c.device, c.hidden, c.radial_bins, c.radial_max_um = device, hidden, radial_bins, radial_max_um
-        c.batch, c.lr, c.radial_weight, c.seed = batch, lr, radial_weight, seed
+        c.batch, c.lr, c.radial_weight, c.seed, c.lateral_um = batch, lr, radial_weight, seed, lateral_um
         self.config = c
         self.radial_bins = radial_bins
         self.radial_max_um = radial_max_um
@@ -180,6 +193,9 @@ class Surrogate:
         tl, vl = ctypes.c_float(), ctypes.c_float()
         self._check(self._lib.fd2_sg_train(self._h, steps, ctypes.byref(tl), ctypes.byref(vl)), "train")
         return float(tl.value), float(vl.value)
+
+    def set_lr(self, lr: float):
+        self._check(self._lib.fd2_sg_set_lr(self._h, lr), "set_lr")
 
     def eval(self) -> dict:
         a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()

@@ -4,18 +4,26 @@ Defaults follow the surrogate-training workload: 2,000,000 points over
 detector geometries drawn from the batched workload's ranges (thickness
 100-600 um, column radius 2.5-7.5 um, roughness 0-0.5, top reflectivity 0-1,
 bulk absorption 1e-5..1e-3 /um), each point a deposition at depth U(0, H)
-with energy U(1, 80) keV labelled by 10,000 Monte Carlo photons (detected
-fraction and a 64-bin radial histogram to 200 um); MLP 8-256-256-256-25,
-BF16 GEMMs with FP32 accumulation, Adam, batch 8,192, 5 % held out.
+with energy U(0.05, 80) keV labelled by 10,000 Monte Carlo photons
+(detected fraction and a 96-bin radial histogram to 400 um, quadratic bin
+edges); MLP 8-256-256-256-25, BF16 GEMMs with FP32 accumulation, Adam with
+a cosine step-size decay, batch 8,192, 5 % held out.
+
+``--focus CONFIG`` continues the training of ``--init`` on depositions in the
+detector of one benchmark configuration only (the detector a simulation
+campaign uses), with the routing hull narrowed to it.
+
 Prints one JSON line with the losses and timings; writes the network with
 ``--out``.
 """
+import math
 import argparse
 import json
 import time
 
 import numpy as np
 
+from . import fastdetect2 as fd
 from . import surrogate as sgm
 
 
@@ -30,24 +38,35 @@ def main():
     ap.add_argument("--val", type=float, default=0.05)
     ap.add_argument("--seed", type=int, default=20240)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--lr-min", type=float, default=1e-5)
+    ap.add_argument("--init", default="")
+    ap.add_argument("--focus", type=int, default=-1)
     ap.add_argument("--out", default="")
     a = ap.parse_args()
     t0 = time.perf_counter()
-    geoms = sgm.sample_geometries(a.geometries, seed=a.seed)
-    per = max(1, a.points // a.geometries)
-    f, ph, det, rad = sgm.label_points(geoms, per, a.photons, seed=a.seed + 1, device=a.device)
+    if a.focus >= 0:
+        geoms = [fd.params_to_geometry(fd.synth_events(a.focus, 1, 1).params)]
+    else:
+        geoms = sgm.sample_geometries(a.geometries, seed=a.seed)
+    per = max(1, a.points // len(geoms))
+    f, ph, det, rad = sgm.label_points(geoms, per, a.photons, seed=a.seed + 1, device=a.device,
+                                       energy_kev=(0.05, 80.0))
     t_label = time.perf_counter() - t0
     perm = np.random.default_rng(a.seed + 2).permutation(len(f))
     f, ph, det, rad = f[perm], ph[perm], det[perm], rad[perm]
     n_val = int(a.val * len(f))
     with sgm.Surrogate(device=a.device, batch=a.batch, lr=a.lr, seed=a.seed + 3) as s:
+        if a.init:
+            s.load(a.init)
         s.set_data(f, ph, det, rad, n_val=n_val)
         before = s.eval()
         t1 = time.perf_counter()
         curve = []
         done = 0
         while done < a.steps:
-            k = min(500, a.steps - done)
+            k = min(250, a.steps - done)
+            frac = (done + 0.5 * k) / a.steps
+            s.set_lr(a.lr_min + 0.5 * (a.lr - a.lr_min) * (1.0 + math.cos(math.pi * frac)))
             tl, vl = s.train(k)
             done += k
             curve.append({"step": done, "train": tl, "val": vl})

@@ -126,10 +126,11 @@ typedef struct fd2_options {
     int32_t fresnel_batch;         /* lanes parked at a column wall before the warp
                                       runs their Fresnel interaction; 0 = tuned   */
     int32_t radial_bins;           /* > 0: label mode -- each history's detected
-                                      photons are binned by distance from their
-                                      event in radial_bins bins up to
-                                      radial_max_um plus one overflow bin
-                                      (fd2_get_radial) instead of the PRF image */
+                                      photons are binned by distance r from their
+                                      event instead of the PRF image: bin j <
+                                      radial_bins covers r_max (j/bins)^2 ..
+                                      r_max ((j+1)/bins)^2, bin radial_bins is
+                                      r >= r_max = radial_max_um (fd2_get_radial) */
     double radial_max_um;
 } fd2_options;
 

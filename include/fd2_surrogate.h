@@ -27,8 +27,12 @@
  *   3 thickness H, um     4 column radius R, um    5 roughness beta
  *   6 top reflectivity (1 - top_absfrac)           7 log10(bulk absorption, 1/um)
  * Network outputs (FD2_SG_OUTPUTS per point): [0] detection logit,
- * [1..8] mixture weight logits, [9..16] means (units of 50 um),
- * [17..24] log widths (width = 10 um * exp(.), clamped to [-6, 4]).
+ * [1..8] weight logits of an 8-component mixture of Gaussian rings
+ * (PRF(r) = sum_k w_k N(r; mu_k, sd_k) / S_k per unit area), [9..16] ring
+ * radii (mu = 50 um * softplus(.)), [17..24] log widths (sd = 10 um *
+ * exp(.), clamped to [-6, 4]).  Radial label categories: bin j <
+ * radial_bins covers r_max (j/bins)^2 .. r_max ((j+1)/bins)^2, the last is
+ * r >= r_max.
  */
 #ifndef FD2_SURROGATE_H
 #define FD2_SURROGATE_H
@@ -48,15 +52,23 @@ typedef struct fd2_sg fd2_sg;
 typedef struct fd2_sg_config {
     int32_t device;
     int32_t hidden;          /* width of the three hidden layers (multiple of 64; 256) */
-    int32_t radial_bins;     /* label histogram bins up to radial_max_um (+1 overflow) */
-    double radial_max_um;    /* 200 */
+    int32_t radial_bins;     /* label histogram bins up to radial_max_um (+1 beyond); 96 */
+    double radial_max_um;    /* 400 */
     int32_t batch;           /* training batch (multiple of 64; 8192) */
     float lr, beta1, beta2, adam_eps;
     float radial_weight;     /* weight of the radial loss beside the detection loss */
+    float lateral_um;        /* fd2_sg_run: depositions farther than this from the
+                                detector centre (in x or y) go to the Monte Carlo;
+                                the labels sit at the centre, so their far light is
+                                what the detector's edges leave from there; 50 */
     uint64_t seed;           /* initialisation and batch sampling */
 } fd2_sg_config;
 
-/* Box of the training data: features outside it go to the Monte Carlo. */
+/* Box of the training data: events whose features lie outside it go to the
+ * Monte Carlo.  The first hull a new network gets (fd2_sg_set_data or
+ * fd2_sg_set_hull) also fixes its input normalisation, which then stays with
+ * the network (saved, loaded); later hulls only change the routing, e.g.
+ * narrowed to the data of a continued training. */
 typedef struct fd2_sg_hull {
     float lo[FD2_SG_FEATURES];
     float hi[FD2_SG_FEATURES];
@@ -89,6 +101,8 @@ FD2_API fd2_status fd2_sg_set_data(fd2_sg *sg, const float *features, const int3
 /* `steps` Adam steps on batches drawn uniformly from the training points;
  * returns the mean training loss of the last steps and the held-out loss. */
 FD2_API fd2_status fd2_sg_train(fd2_sg *sg, int32_t steps, float *train_loss, float *val_loss);
+/* Adam step size of the following training steps (schedules). */
+FD2_API fd2_status fd2_sg_set_lr(fd2_sg *sg, float lr);
 /* Loss on the held-out points (or all points when n_val = 0). */
 FD2_API fd2_status fd2_sg_eval(fd2_sg *sg, float *loss, float *det_loss, float *radial_loss);
 

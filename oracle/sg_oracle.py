@@ -7,6 +7,10 @@ FP64, the network and loss that include/fd2_surrogate.h documents:
   x   = 2 (f - lo) / (hi - lo) - 1          (8 features; constant features -> 0)
   h1  = relu(x W1^T + b1), h2 = relu(h1 W2^T + b2), h3 = relu(h2 W3^T + b3)
   out = h3 W4^T + b4                         (25 outputs)
+  mixture of Gaussian rings: PRF(r) = sum_k w_k N(r; mu_k, sd_k) / S_k per
+           unit area, w = softmax(out[1..8]), mu = 50 um softplus(out[9..16]),
+           sd = 10 um exp(clamp(out[17..24], -6, 4));
+  radial categories: quadratic edges r_max (j/bins)^2, then r >= r_max
   L   = mean_i [ BCE(sigmoid(out0), d/N) + lambda * CE(y, q(out)) ]
 
 With ``bf16=True`` it rounds to BF16 exactly where the GPU stores BF16 (the
@@ -69,9 +73,21 @@ def forward(p, hidden, f, lo, hi, bf=True):
     return out, (x, h1, h2, h3, Ws)
 
 
-def point_loss(out, t, y, bins, width, lam):
-    """Loss of every row and dL/dout (rows of 25); y None rows have no
-    radial term (y rows all zero)."""
+def _ring(mu, sd, e, inf):
+    """Edge values of ring components: t, Phi, Phi_c, phi, e (arrays [..., E])."""
+    t = np.where(inf, 0.0, (e - mu) / sd)
+    cdf = np.where(inf, 1.0, ndtr(t))
+    ccdf = np.where(inf, 0.0, ndtr(-t))
+    pdf = np.where(inf, 0.0, np.exp(-0.5 * t * t) / np.sqrt(2 * np.pi))
+    return t, cdf, ccdf, pdf, np.where(inf, 0.0, e)
+
+
+def point_loss(out, t, y, bins, r_max, lam):
+    """Loss of every row and dL/dout (rows of 25); rows whose y is all zero
+    have no radial term.  Radial model: mixture of Gaussian rings, component
+    k's radial density r N(r; mu_k, sd_k) / S_k on r >= 0; bin masses
+    M(a, b) = mu [Phi(t_b) - Phi(t_a)] + sd [phi(t_a) - phi(t_b)]; quadratic
+    bin edges r_max (j / bins)^2 and a last category beyond r_max."""
     n = out.shape[0]
     z = out[:, 0]
     p = 1.0 / (1.0 + np.exp(-z))
@@ -83,37 +99,45 @@ def point_loss(out, t, y, bins, width, lam):
     a = out[:, 1:1 + K]
     w = np.exp(a - a.max(1, keepdims=True))
     w /= w.sum(1, keepdims=True)
-    mu = MU_SCALE * out[:, 1 + K:1 + 2 * K]
+    om = out[:, 1 + K:1 + 2 * K]
+    mu = MU_SCALE * (np.maximum(om, 0) + np.log1p(np.exp(-np.abs(om))))
+    dmu = MU_SCALE / (1.0 + np.exp(-om))
     ls = out[:, 1 + 2 * K:1 + 3 * K]
     clamped = (ls < LOG_SD_MIN) | (ls > LOG_SD_MAX)
     sd = SD_SCALE * np.exp(np.clip(ls, LOG_SD_MIN, LOG_SD_MAX))
-    edges = np.arange(bins + 1) * width
-    aa = (edges[None, None, :] - mu[:, :, None]) / sd[:, :, None]        # [n, K, bins+1]
-    a_all = np.concatenate([aa, np.full((n, K, 1), np.inf)], axis=2)     # last edge +inf
-    cdf = ndtr(a_all)
-    ccdf = ndtr(-a_all)
-    pdf = np.where(np.isinf(a_all), 0.0, np.exp(-0.5 * np.where(np.isinf(a_all), 0, a_all) ** 2) / np.sqrt(2 * np.pi))
-    apdf = np.where(np.isinf(a_all), 0.0, np.where(np.isinf(a_all), 0, a_all) * pdf)
-    # lower-tail differences left of the mean, upper-tail ones right of it
-    a_lo = a_all[:, :, :-1]
-    P = np.maximum(np.where(a_lo >= 0, ccdf[:, :, :-1] - ccdf[:, :, 1:], cdf[:, :, 1:] - cdf[:, :, :-1]), 0.0)
-    a0 = -mu / sd
-    S = ndtr(-a0)
-    Z = np.maximum((w * S).sum(1), 1e-30)
-    A = (w[:, :, None] * P).sum(1)                                       # [n, bins+1]
+    edges = r_max * (np.arange(bins + 1) / bins) ** 2
+    E = np.concatenate([edges, [0.0]])                       # bins + 2 edges, the last is +inf
+    inf = np.zeros(bins + 2, bool)
+    inf[-1] = True
+    mu3, sd3 = mu[:, :, None], sd[:, :, None]
+    tt, cdf, ccdf, pdf, ee = _ring(mu3, sd3, E[None, None, :], inf[None, None, :])
+    tlo, thi = tt[:, :, :-1], tt[:, :, 1:]
+    dphi = np.maximum(np.where((tlo >= 0) & ~inf[None, None, :-1], ccdf[:, :, :-1] - ccdf[:, :, 1:],
+                               cdf[:, :, 1:] - cdf[:, :, :-1]), 0.0)
+    plo, phi_ = pdf[:, :, :-1], pdf[:, :, 1:]
+    elo, ehi = ee[:, :, :-1], ee[:, :, 1:]
+    M = np.maximum(mu3 * dphi + sd3 * (plo - phi_), 0.0)       # [n, K, bins+1]
+    dM_mu = dphi + (elo * plo - ehi * phi_) / sd3
+    dM_sd = (plo - phi_) + (tlo * elo * plo - thi * ehi * phi_) / sd3
+    t0 = -mu / sd
+    c0 = ndtr(-t0)
+    p0 = np.exp(-0.5 * t0 * t0) / np.sqrt(2 * np.pi)
+    S = np.maximum(mu * c0 + sd * p0, 1e-30)
+    q = (w[:, :, None] * M / S[:, :, None]).sum(1)             # [n, bins+1]
+    qe = q + 1e-12
     has = y.sum(1) > 0
-    Ae = A + 1e-12
-    lr = np.log(Z) - (y * np.log(Ae)).sum(1)
-    c = y / Ae
-    phi0 = np.exp(-0.5 * a0 ** 2) / np.sqrt(2 * np.pi)
-    gw = S / Z[:, None] - (c[:, None, :] * P).sum(2)
-    dPdmu = -(pdf[:, :, 1:] - pdf[:, :, :-1]) / sd[:, :, None]
-    dPdsd = -(apdf[:, :, 1:] - apdf[:, :, :-1]) / sd[:, :, None]
-    gmu = w / Z[:, None] * phi0 / sd - w * (c[:, None, :] * dPdmu).sum(2)
-    gsd = w / Z[:, None] * a0 * phi0 / sd - w * (c[:, None, :] * dPdsd).sum(2)
+    lr = -(y * np.log(qe)).sum(1)
+    c = y / qe
+    A1 = (c[:, None, :] * M).sum(2)
+    Amu = (c[:, None, :] * dM_mu).sum(2)
+    Asd = (c[:, None, :] * dM_sd).sum(2)
+    gw = -A1 / S
+    f = w / S
+    gmu = -f * (Amu - A1 * c0 / S)
+    gsd = -f * (Asd - A1 * p0 / S)
     wg = (w * gw).sum(1, keepdims=True)
     g[:, 1:1 + K] = lam * w * (gw - wg)
-    g[:, 1 + K:1 + 2 * K] = lam * MU_SCALE * gmu
+    g[:, 1 + K:1 + 2 * K] = lam * dmu * gmu
     g[:, 1 + 2 * K:] = np.where(clamped, 0.0, lam * sd * gsd)
     g[~has, 1:] = 0.0
     lr = np.where(has, lr, 0.0)
@@ -137,7 +161,7 @@ def loss_grad(p, hidden, f, lo, hi, photons, detected, radial, bins=64, radial_m
     if bf:
         out = out.astype(np.float32).astype(np.float64)
     t, y = labels(photons, detected, radial)
-    L, g, _, _ = point_loss(out, t, y, bins, radial_max / bins, lam)
+    L, g, _, _ = point_loss(out, t, y, bins, radial_max, lam)
     n = out.shape[0]
     dout = r(g / n)
     dW4 = dout.T @ h3
@@ -157,5 +181,5 @@ def loss_grad(p, hidden, f, lo, hi, photons, detected, radial, bins=64, radial_m
 def loss_only(p, hidden, f, lo, hi, photons, detected, radial, bins=64, radial_max=200.0, lam=1.0):
     out, _ = forward(p, hidden, f, lo, hi, bf=False)
     t, y = labels(photons, detected, radial)
-    L, _, _, _ = point_loss(out, t, y, bins, radial_max / bins, lam)
+    L, _, _, _ = point_loss(out, t, y, bins, radial_max, lam)
     return float(L.mean())

@@ -45,7 +45,7 @@ def _random_problem(seed, n, hidden):
 def test_gradients_match_oracle(require_gpu):
     H, n = 64, 192
     p, f, lo, hi, ph, de, ra = _random_problem(11, n, H)
-    with sgm.Surrogate(hidden=H, batch=256) as s:
+    with sgm.Surrogate(hidden=H, batch=256, radial_bins=64, radial_max_um=200.0) as s:
         s.set_params(p)
         s.set_hull(lo, hi)
         assert np.array_equal(s.params(), p)
@@ -65,7 +65,7 @@ def test_gradients_match_oracle(require_gpu):
 def test_label_mode_counts_every_detected_photon(require_gpu):
     geoms = sgm.sample_geometries(3, seed=5)
     f, ph, det, rad = sgm.label_points(geoms, 40, 1500, seed=9)
-    assert f.shape == (120, 8) and rad.shape == (120, 65)
+    assert f.shape == (120, 8) and rad.shape == (120, 97)
     assert np.array_equal(det, rad.sum(1).astype(np.int32))
     assert np.all(det <= ph) and 0.02 < det.sum() / ph.sum() < 0.98
     # the same photons without label mode: identical per-history counts
