@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             // crosstalk: one attempt at the next column's normal per round, so
             // a rejected attempt is retried beside the other lanes' first ones
             if (xretry || fate == kNeedsNormal) {
+                w.top_up();  // warp-wide refill for fresh and retried attempts alike
                 fate = kMulti ? w.crosstalk_normal(s_geom[geom], xtries) : w.crosstalk_normal(a.g0, xtries);
                 xretry = fate == kRetryNormal;
                 if (xretry) fate = kAlive;
@@ -476,6 +477,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             const unsigned busy = __ballot_sync(kFull, alive && !parked && fate == kAlive);
             if ((unsigned)__popc(waiting) >= fresnel_min || busy == 0) {
                 if (parked) {
+                    w.top_up();  // the parked lanes' rings, refilled together
                     fate = kMulti ? w.surface_fresnel(s_geom[geom]) : w.surface_fresnel(a.g0);
                     parked = false;
                 }
