@@ -24,6 +24,7 @@ STATUS_NAMES = {
 }
 COUNT_POISSON, COUNT_GAUSSIAN, COUNT_GIVEN = 0, 1, 2
 REPLAY_REF, REPLAY_FP64 = 0, 1
+UNITS_CM, UNITS_UM = 0, 1
 
 
 class Fd2Error(RuntimeError):
@@ -88,6 +89,15 @@ class Timing(ctypes.Structure):
                 ("refill", ctypes.c_int32), ("prf_window", ctypes.c_int32), ("fresnel_batch", ctypes.c_int32)]
 
 
+class IngestStats(ctypes.Structure):
+    _fields_ = [("events", ctypes.c_int64), ("batches", ctypes.c_int64), ("photons", ctypes.c_int64),
+                ("host_seconds", ctypes.c_double), ("push_wait_seconds", ctypes.c_double),
+                ("device_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class Events(ctypes.Structure):
     _fields_ = [
         ("n", ctypes.c_int64), ("num_hist", ctypes.c_int32),
@@ -133,6 +143,7 @@ EXPORTED = [
     "fd2_autotune", "fd2_transport_noalloc",
     "fd2_synth_events", "fd2_free_events", "fd2_read_events_text", "fd2_write_events_text",
     "fd2_read_events_binary", "fd2_write_events_binary",
+    "fd2_ingest_begin", "fd2_ingest_push", "fd2_ingest_push_um", "fd2_ingest_file", "fd2_ingest_end",
     "gpuoptical_", "cpuoptical_", "gpuoptlb_", "cpuoptlb_", "fd2_compat_status",
     "fd2_sg_default_config", "fd2_sg_create", "fd2_sg_destroy", "fd2_sg_last_error", "fd2_sg_set_data",
     "fd2_sg_train", "fd2_sg_set_lr", "fd2_sg_eval", "fd2_sg_num_params", "fd2_sg_get_params", "fd2_sg_set_params",
@@ -191,6 +202,11 @@ def load():
         "fd2_write_events_text": (ctypes.c_int, [ctypes.c_char_p, P(Events)]),
         "fd2_read_events_binary": (ctypes.c_int, [ctypes.c_char_p, P(Events)]),
         "fd2_write_events_binary": (ctypes.c_int, [ctypes.c_char_p, P(Events)]),
+        "fd2_ingest_begin": (ctypes.c_int, [vp, ctypes.c_int64, ctypes.c_int32, P(vp)]),
+        "fd2_ingest_push": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int64]),
+        "fd2_ingest_push_um": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int64]),
+        "fd2_ingest_file": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "fd2_ingest_end": (ctypes.c_int, [vp, P(IngestStats)]),
         "fd2_compat_status": (ctypes.c_int, []),
         "fd2_sg_default_config": (None, [P(SgConfig)]),
         "fd2_sg_create": (ctypes.c_int, [P(SgConfig), P(vp)]),

@@ -464,6 +464,11 @@ cudaError_t count_pass(fd2_ctx *c, bool for_transport) { return ::count_pass(c, 
 cudaError_t enqueue_segment(fd2_ctx *c, int seg) { return ::enqueue_segment(c, seg); }
 TransportArgs transport_args(fd2_ctx *c) { return ::transport_args(c); }
 fd2_status ensure_chunks(fd2_ctx *c) { return ::ensure_chunks(c); }
+fd2_status ensure_events(fd2_ctx *c, int64_t n) { return ::ensure_events(c, n); }
+void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *geom, int64_t n)
+{
+    ::choose_window(c, x, y, geom, n);
+}
 fd2_status check_status(fd2_ctx *c) { return ::check_status(c); }
 fd2_status fail(fd2_ctx *c, fd2_status s, const std::string &msg) { return ::fail(c, s, msg); }
 
@@ -585,6 +590,7 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
 void fd2_destroy(fd2_ctx *c)
 {
     if (!c) return;
+    if (c->ingest) fd2_ingest_end(c->ingest, nullptr);
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto g : c->graph)
@@ -624,6 +630,7 @@ void fd2_destroy(fd2_ctx *c)
 
 fd2_status fd2_set_geometries(fd2_ctx *c, const fd2_geometry *g, int32_t n)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c || !g || n <= 0 || n > 256) return fail(c, FD2_ERR_INVALID_ARGUMENT, "1..256 geometries");
     for (int32_t i = 0; i < n; ++i)
         if (!valid_geometry(g[i])) return fail(c, FD2_ERR_INVALID_ARGUMENT, "invalid geometry " + std::to_string(i));
@@ -672,6 +679,7 @@ static fd2_status submit_common(fd2_ctx *c, int64_t n, const float *xs, const fl
 fd2_status fd2_submit_events(fd2_ctx *c, const double *x_cm, const double *y_cm, const double *z_cm, const double *de_ev,
                              const int32_t *hist, int64_t n)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c || n < 0 || (n > 0 && (!x_cm || !y_cm || !z_cm || !de_ev || !hist)) || n >= ((int64_t)1 << 31))
         return fail(c, FD2_ERR_INVALID_ARGUMENT, "submit_events: null array or bad count");
     if (c->run_pending) {
@@ -713,6 +721,7 @@ fd2_status fd2_submit_events(fd2_ctx *c, const double *x_cm, const double *y_cm,
 fd2_status fd2_submit_events_um(fd2_ctx *c, const float *x_um, const float *y_um, const float *z_um, const float *e_ev,
                                 const int32_t *hist, const int32_t *nphot, const uint16_t *geom, int64_t n)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c || n < 0 || (n > 0 && (!x_um || !y_um || !z_um || !hist)) || n >= ((int64_t)1 << 31))
         return fail(c, FD2_ERR_INVALID_ARGUMENT, "submit_events_um: null array or bad count");
     if (c->run_pending) {
@@ -778,6 +787,7 @@ fd2_status fd2_submit_events_um(fd2_ctx *c, const float *x_um, const float *y_um
 
 fd2_status fd2_run(fd2_ctx *c)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c) return FD2_ERR_INVALID_ARGUMENT;
     if (c->n_events <= 0 && !c->ran_once && c->cap_events == 0) return fail(c, FD2_ERR_STATE, "no events submitted");
     FD2_CUDA(c, cudaSetDevice(c->device));
@@ -836,6 +846,7 @@ fd2_status fd2_wait(fd2_ctx *c)
 
 fd2_status fd2_reset_tallies(fd2_ctx *c)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c) return FD2_ERR_INVALID_ARGUMENT;
     if (c->run_pending) return fail(c, FD2_ERR_STATE, "wait first");
     FD2_CUDA(c, cudaSetDevice(c->device));
@@ -1009,6 +1020,7 @@ fd2_status fd2_write_outputs(fd2_ctx *c, const char *dir)
 fd2_status fd2_replay(fd2_ctx *c, int32_t mode, int32_t seed_input, int64_t event_index_base, int8_t *fate,
                       int32_t *pix, int32_t *seeds, int32_t *steps)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c || (mode != FD2_REPLAY_REF && mode != FD2_REPLAY_FP64) || seed_input <= 0 || event_index_base < 0)
         return fail(c, FD2_ERR_INVALID_ARGUMENT, "replay mode / seed");
     fd2_status st = fd2_wait(c);
@@ -1075,6 +1087,7 @@ fd2_status fd2_replay(fd2_ctx *c, int32_t mode, int32_t seed_input, int64_t even
 
 fd2_status fd2_autotune(fd2_ctx *c, int32_t budget_runs)
 {
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c) return FD2_ERR_INVALID_ARGUMENT;
     if (c->n_events <= 0) return fail(c, FD2_ERR_STATE, "submit events before tuning");
     fd2_status st = fd2_wait(c);

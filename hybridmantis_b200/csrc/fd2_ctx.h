@@ -67,6 +67,8 @@ struct fd2_ctx {
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     bool graph_valid = false;
     bool run_pending = false, ran_once = false;
+    bool ingest_active = false;  // fd2_ingest_begin .. fd2_ingest_end
+    fd2_ingest *ingest = nullptr; // the open ingest, ended by fd2_destroy
     fd2::TransportConfig cfg;
     int win_x0 = 0, win_y0 = 0;
     int64_t last_photons = 0;
@@ -84,6 +86,8 @@ cudaError_t count_pass(fd2_ctx *c, bool for_transport);   // photon counts + chu
 cudaError_t enqueue_segment(fd2_ctx *c, int seg);         // 0 counts+queue, 1 transport, 2 PHS + run tag
 TransportArgs transport_args(fd2_ctx *c);
 fd2_status ensure_chunks(fd2_ctx *c);
+fd2_status ensure_events(fd2_ctx *c, int64_t n);
+void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *geom, int64_t n);
 fd2_status check_status(fd2_ctx *c);
 fd2_status fail(fd2_ctx *c, fd2_status s, const std::string &msg);
 

@@ -7,6 +7,7 @@
 //   detected_<tags>.dat     418-458 (names, (1x,F12.4) blocks, (1x,I8) rows)
 //   EDE text rows           the tally's event write (3(1x,1pe16.9),1x,1pe12.4,i8)
 //                           in cm / eV / 1-based history, :173-174
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -168,40 +169,23 @@ void fd2_free_events(fd2_events *ev)
 fd2_status fd2_read_events_text(const char *path, fd2_events *out)
 {
     if (!path || !out) return FD2_ERR_INVALID_ARGUMENT;
-    FILE *f = std::fopen(path, "r");
-    if (!f) return FD2_ERR_IO;
     std::vector<float> x, y, z, e;
     std::vector<int32_t> h;
-    char line[1024];
     int32_t max_hist = 0;
-    fd2_status st = FD2_OK;
-    while (std::fgets(line, sizeof line, f)) {
-        const char *s = line;
-        while (*s == ' ' || *s == '\t') ++s;
-        if (*s == '#' || *s == '\0' || *s == '\n' || *s == '\r') continue;
-        char buf[5][64];
-        if (std::sscanf(s, "%63s %63s %63s %63s %63s", buf[0], buf[1], buf[2], buf[3], buf[4]) != 5) {
-            st = FD2_ERR_PARSE;
-            break;
-        }
-        double v[4];
-        int32_t hh = 0;
-        bool ok = true;
-        for (int k = 0; k < 4; ++k) ok = ok && parse_real(buf[k], &v[k]);
-        ok = ok && parse_int(buf[4], &hh);
-        if (!ok) {
-            st = FD2_ERR_PARSE;
-            break;
-        }
-        // cm -> um as the reference's host driver does (double * 10000.0f)
-        x.push_back((float)(v[0] * (double)10000.0f));
-        y.push_back((float)(v[1] * (double)10000.0f));
-        z.push_back((float)(v[2] * (double)10000.0f));
-        e.push_back((float)v[3]);
-        h.push_back(hh);
-        if (hh > max_hist) max_hist = hh;
-    }
-    std::fclose(f);
+    const fd2_status st = fd2host::stream_events_text(
+        path, 1 << 16,
+        [&](const double *xc, const double *yc, const double *zc, const double *de, const int32_t *hh, int64_t n) {
+            for (int64_t i = 0; i < n; ++i) {
+                // cm -> um as the reference's host driver does (double * 10000.0f)
+                x.push_back((float)(xc[i] * (double)10000.0f));
+                y.push_back((float)(yc[i] * (double)10000.0f));
+                z.push_back((float)(zc[i] * (double)10000.0f));
+                e.push_back((float)de[i]);
+                h.push_back(hh[i]);
+                if (hh[i] > max_hist) max_hist = hh[i];
+            }
+            return FD2_OK;
+        });
     if (st != FD2_OK) return st;
     return fd2host::events_from_vectors(x, y, z, e, h, max_hist, out);
 }
@@ -240,43 +224,40 @@ fd2_status fd2_write_events_binary(const char *path, const fd2_events *ev)
 fd2_status fd2_read_events_binary(const char *path, fd2_events *out)
 {
     if (!path || !out) return FD2_ERR_INVALID_ARGUMENT;
-    FILE *f = std::fopen(path, "rb");
-    if (!f) return FD2_ERR_IO;
-    char magic[8];
-    int64_t n = 0;
-    int32_t num_hist = 0, has_geom = 0;
-    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kBinMagic, 8) == 0 &&
-              std::fread(&n, 8, 1, f) == 1 && std::fread(&num_hist, 4, 1, f) == 1 &&
-              std::fread(&has_geom, 4, 1, f) == 1 && n >= 0 && n < (int64_t)1 << 34;
-    if (!ok) {
-        std::fclose(f);
-        return FD2_ERR_PARSE;
-    }
     fd2_events ev;
     std::memset(&ev, 0, sizeof ev);
-    ev.n = n;
-    ev.num_hist = num_hist;
-    ev.num_geom = 1;
-    const size_t N = (size_t)n ? (size_t)n : 1;
-    ev.x_um = (float *)std::malloc(4 * N);
-    ev.y_um = (float *)std::malloc(4 * N);
-    ev.z_um = (float *)std::malloc(4 * N);
-    ev.e_ev = (float *)std::malloc(4 * N);
-    ev.hist = (int32_t *)std::malloc(4 * N);
-    if (has_geom) ev.geom = (uint16_t *)std::malloc(2 * N);
-    if (!ev.x_um || !ev.y_um || !ev.z_um || !ev.e_ev || !ev.hist || (has_geom && !ev.geom)) {
-        std::fclose(f);
+    int64_t at = 0;
+    const fd2_status st = fd2host::stream_events_binary(
+        path, 1 << 20,
+        [&](const fd2host::BinHeader &hd) {
+            ev.n = hd.n;
+            ev.num_hist = hd.num_hist;
+            ev.num_geom = 1;
+            const size_t N = (size_t)hd.n ? (size_t)hd.n : 1;
+            ev.x_um = (float *)std::malloc(4 * N);
+            ev.y_um = (float *)std::malloc(4 * N);
+            ev.z_um = (float *)std::malloc(4 * N);
+            ev.e_ev = (float *)std::malloc(4 * N);
+            ev.hist = (int32_t *)std::malloc(4 * N);
+            if (hd.has_geom) ev.geom = (uint16_t *)std::malloc(2 * N);
+            if (!ev.x_um || !ev.y_um || !ev.z_um || !ev.e_ev || !ev.hist || (hd.has_geom && !ev.geom))
+                return FD2_ERR_OUT_OF_MEMORY;
+            return FD2_OK;
+        },
+        [&](const float *x, const float *y, const float *z, const float *e, const int32_t *h, const uint16_t *g,
+            int64_t n) {
+            std::memcpy(ev.x_um + at, x, 4 * (size_t)n);
+            std::memcpy(ev.y_um + at, y, 4 * (size_t)n);
+            std::memcpy(ev.z_um + at, z, 4 * (size_t)n);
+            std::memcpy(ev.e_ev + at, e, 4 * (size_t)n);
+            std::memcpy(ev.hist + at, h, 4 * (size_t)n);
+            if (g && ev.geom) std::memcpy(ev.geom + at, g, 2 * (size_t)n);
+            at += n;
+            return FD2_OK;
+        });
+    if (st != FD2_OK) {
         fd2_free_events(&ev);
-        return FD2_ERR_OUT_OF_MEMORY;
-    }
-    ok = std::fread(ev.x_um, 4, (size_t)n, f) == (size_t)n && std::fread(ev.y_um, 4, (size_t)n, f) == (size_t)n &&
-         std::fread(ev.z_um, 4, (size_t)n, f) == (size_t)n && std::fread(ev.e_ev, 4, (size_t)n, f) == (size_t)n &&
-         std::fread(ev.hist, 4, (size_t)n, f) == (size_t)n;
-    if (ok && has_geom) ok = std::fread(ev.geom, 2, (size_t)n, f) == (size_t)n;
-    std::fclose(f);
-    if (!ok) {
-        fd2_free_events(&ev);
-        return FD2_ERR_PARSE;
+        return st;
     }
     *out = ev;
     return FD2_OK;
@@ -415,6 +396,175 @@ fd2_status write_new_file(const std::string &path, const std::string &data)
         off += (size_t)w;
     }
     return ::close(fd) == 0 ? FD2_OK : FD2_ERR_IO;
+}
+
+// ---- streaming EDE readers
+
+namespace {
+
+// One whitespace-delimited token of at most 63 characters as a real; a
+// Fortran 'd' exponent is read as 'e' (parse_real's rule, without a copy to
+// the heap).
+bool token_real(const char *t, size_t len, double *out)
+{
+    char b[64];
+    if (len == 0 || len >= sizeof b) return false;
+    for (size_t k = 0; k < len; ++k) b[k] = (t[k] == 'd' || t[k] == 'D') ? 'e' : t[k];
+    b[len] = '\0';
+    char *end = nullptr;
+    errno = 0;
+    const double v = std::strtod(b, &end);
+    if (end != b + len || errno == ERANGE) return false;
+    *out = v;
+    return true;
+}
+
+bool token_int(const char *t, size_t len, int32_t *out)
+{
+    char b[64];
+    if (len == 0 || len >= sizeof b) return false;
+    std::memcpy(b, t, len);
+    b[len] = '\0';
+    char *end = nullptr;
+    errno = 0;
+    const long v = std::strtol(b, &end, 10);
+    if (end != b + len || errno == ERANGE || v < INT32_MIN || v > INT32_MAX) return false;
+    *out = (int32_t)v;
+    return true;
+}
+
+inline bool blank(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+// 1: an event row, 0: a comment or blank line, -1: a malformed row.  The
+// first five tokens are read; more are ignored.
+int parse_row(const char *s, double v[4], int32_t *hist)
+{
+    while (blank(*s)) ++s;
+    if (*s == '#' || *s == '\0') return 0;
+    const char *tok[5];
+    size_t len[5];
+    for (int k = 0; k < 5; ++k) {
+        while (blank(*s)) ++s;
+        if (*s == '\0') return -1;
+        tok[k] = s;
+        while (*s && !blank(*s)) ++s;
+        len[k] = (size_t)(s - tok[k]);
+    }
+    for (int k = 0; k < 4; ++k)
+        if (!token_real(tok[k], len[k], &v[k])) return -1;
+    return token_int(tok[4], len[4], hist) ? 1 : -1;
+}
+
+}  // namespace
+
+fd2_status stream_events_text(const char *path, int64_t batch, const TextSink &sink)
+{
+    if (!path || batch <= 0) return FD2_ERR_INVALID_ARGUMENT;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return FD2_ERR_IO;
+    const size_t cap = (size_t)batch;
+    std::vector<double> x(cap), y(cap), z(cap), e(cap);
+    std::vector<int32_t> h(cap);
+    size_t fill = 0;
+    std::vector<char> buf((size_t)1 << 22);
+    size_t have = 0;
+    bool eof = false;
+    fd2_status st = FD2_OK;
+    auto row = [&](const char *line) {
+        double v[4];
+        int32_t hh = 0;
+        const int r = parse_row(line, v, &hh);
+        if (r < 0) return FD2_ERR_PARSE;
+        if (r == 0) return FD2_OK;
+        x[fill] = v[0];
+        y[fill] = v[1];
+        z[fill] = v[2];
+        e[fill] = v[3];
+        h[fill] = hh;
+        if (++fill == cap) {
+            fill = 0;
+            return sink(x.data(), y.data(), z.data(), e.data(), h.data(), (int64_t)cap);
+        }
+        return FD2_OK;
+    };
+    while (st == FD2_OK) {
+        if (!eof) {
+            const size_t r = std::fread(buf.data() + have, 1, buf.size() - 1 - have, f);
+            if (r == 0) {
+                if (std::ferror(f)) st = FD2_ERR_IO;
+                eof = true;
+            }
+            have += r;
+        }
+        size_t start = 0;
+        while (st == FD2_OK) {
+            char *nl = (char *)std::memchr(buf.data() + start, '\n', have - start);
+            if (!nl) break;
+            *nl = '\0';
+            st = row(buf.data() + start);
+            start = (size_t)(nl - buf.data()) + 1;
+        }
+        if (st != FD2_OK) break;
+        if (eof) {
+            if (start < have) {  // last row without a newline
+                buf[have] = '\0';
+                st = row(buf.data() + start);
+            }
+            break;
+        }
+        if (start == 0 && have == buf.size() - 1) {
+            st = FD2_ERR_PARSE;  // a row longer than the read buffer
+            break;
+        }
+        std::memmove(buf.data(), buf.data() + start, have - start);
+        have -= start;
+    }
+    std::fclose(f);
+    if (st == FD2_OK && fill > 0) st = sink(x.data(), y.data(), z.data(), e.data(), h.data(), (int64_t)fill);
+    return st;
+}
+
+fd2_status stream_events_binary(const char *path, int64_t batch, const BinHeaderSink &on_header,
+                                const BinSink &sink)
+{
+    if (!path || batch <= 0) return FD2_ERR_INVALID_ARGUMENT;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return FD2_ERR_IO;
+    char magic[8];
+    BinHeader hd{};
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kBinMagic, 8) == 0 &&
+              std::fread(&hd.n, 8, 1, f) == 1 && std::fread(&hd.num_hist, 4, 1, f) == 1 &&
+              std::fread(&hd.has_geom, 4, 1, f) == 1 && hd.n >= 0 && hd.n < (int64_t)1 << 34;
+    if (!ok) {
+        std::fclose(f);
+        return FD2_ERR_PARSE;
+    }
+    fd2_status st = on_header ? on_header(hd) : FD2_OK;
+    const size_t cap = (size_t)std::min<int64_t>(batch, std::max<int64_t>(hd.n, 1));
+    std::vector<float> plane[4];
+    for (auto &v : plane) v.resize(cap);
+    std::vector<int32_t> h(cap);
+    std::vector<uint16_t> g(hd.has_geom ? cap : 0);
+    const int64_t off0 = 24;  // magic, n, num_hist, has_geom
+    for (int64_t i = 0; st == FD2_OK && i < hd.n; i += (int64_t)cap) {
+        const size_t k = (size_t)std::min<int64_t>((int64_t)cap, hd.n - i);
+        // planes x, y, z, e, hist (4 bytes each), then geometry ids (2 bytes)
+        for (int p = 0; ok && p < 5; ++p) {
+            void *dst = p < 4 ? (void *)plane[p].data() : (void *)h.data();
+            ok = fseeko(f, (off_t)(off0 + (int64_t)p * hd.n * 4 + i * 4), SEEK_SET) == 0 &&
+                 std::fread(dst, 4, k, f) == k;
+        }
+        if (ok && hd.has_geom)
+            ok = fseeko(f, (off_t)(off0 + 5 * hd.n * 4 + i * 2), SEEK_SET) == 0 && std::fread(g.data(), 2, k, f) == k;
+        if (!ok) {
+            st = FD2_ERR_PARSE;
+            break;
+        }
+        st = sink(plane[0].data(), plane[1].data(), plane[2].data(), plane[3].data(), h.data(),
+                  hd.has_geom ? g.data() : nullptr, (int64_t)k);
+    }
+    std::fclose(f);
+    return st;
 }
 
 }  // namespace fd2host

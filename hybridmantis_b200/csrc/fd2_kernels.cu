@@ -162,6 +162,14 @@ __global__ void count_kernel(int64_t n, int64_t event_base, int mode, double yie
             atomicOr(status, kStatusTooManyPhotons);
             k = 0;
         }
+        // an event the preparation flagged (non-finite, negative energy,
+        // history outside 1..num_hist) gets no photons: a streamed ingest
+        // queues its transport before the host sees the flag
+        const float4 p = ev_pos[i];
+        const int32_t prim = __float_as_int(p.w);
+        const double e = ev_e ? ev_e[i] : 0.0;  // no energies with given counts (fd2_transport_noalloc)
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(e)) || e < 0.0 || prim < 0 || prim >= n_prim)
+            k = 0;
         ev_n[i] = (int32_t)k;
         ev_nchunks[i] = (uint32_t)((k + chunk - 1) / chunk);
         const int g = ev_geom ? ev_geom[i] : 0;
@@ -169,7 +177,6 @@ __global__ void count_kernel(int64_t n, int64_t event_base, int mode, double yie
             atomicAdd(&photons_per_geom[g], (unsigned long long)k);
             if (photons_total) atomicAdd(&photons_total[g], (unsigned long long)k);
         }
-        const int32_t prim = __float_as_int(ev_pos[i].w);
         if (prim_geom && prim >= 0 && prim < n_prim) prim_geom[prim] = g;
     }
 }
@@ -498,7 +505,8 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             const unsigned det = __ballot_sync(kFull, fate == kDetect);
             if (fate == kDetect) {
                 const unsigned peers = __match_any_sync(det, prim);
-                if (lane == __ffs(peers) - 1 && prim < a.n_prim) atomicAdd(&a.per_primary[prim], __popc(peers));
+                if (lane == __ffs(peers) - 1 && (unsigned)prim < (unsigned)a.n_prim)
+                    atomicAdd(&a.per_primary[prim], __popc(peers));
                 const int xdim = kMulti ? s_geom[geom].xdim : a.g0.xdim;
                 const int ydim = kMulti ? s_geom[geom].ydim : a.g0.ydim;
                 if (kRadial) {
@@ -507,7 +515,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                     const float rr = sqrtf(rx * rx + ry * ry) * a.radial_inv_max;
                     const int b = rr < 1.0f ? min((int)(sqrtf(rr) * (float)a.radial_bins), a.radial_bins - 1)
                                             : a.radial_bins;
-                    if (prim < a.n_prim && b >= 0)
+                    if ((unsigned)prim < (unsigned)a.n_prim && b >= 0)
                         atomicAdd(&a.radial[(long long)prim * (a.radial_bins + 1) + b], 1u);
                 } else if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {
                     atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);

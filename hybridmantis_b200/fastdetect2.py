@@ -16,12 +16,12 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import (COUNT_GAUSSIAN, COUNT_GIVEN, COUNT_POISSON, REPLAY_FP64, REPLAY_REF, Counters,
-                   Fd2Error, Geometry, Options, Params, PhsStats, Timing, check, load, ptr)
+from ._lib import (COUNT_GAUSSIAN, COUNT_GIVEN, COUNT_POISSON, REPLAY_FP64, REPLAY_REF, UNITS_CM, UNITS_UM,
+                   Counters, Fd2Error, Geometry, IngestStats, Options, Params, PhsStats, Timing, check, load, ptr)
 
 __all__ = ["read_input_file", "default_params", "params_to_geometry", "prf_dims", "EventSet", "synth_events",
            "OpticalTransport", "Fd2Error", "COUNT_POISSON", "COUNT_GAUSSIAN", "COUNT_GIVEN",
-           "REPLAY_REF", "REPLAY_FP64", "write_output_files", "read_events_text", "write_events_text", "read_events_binary",
+           "REPLAY_REF", "REPLAY_FP64", "UNITS_CM", "UNITS_UM", "Ingest", "write_output_files", "read_events_text", "write_events_text", "read_events_binary",
            "write_events_binary"]
 
 
@@ -238,6 +238,14 @@ class OpticalTransport:
     def submit(self, es: EventSet, nphot=None):
         self.submit_events_um(es.x_um, es.y_um, es.z_um, es.e_ev, es.hist, nphot, es.geom)
 
+    def ingest(self, batch_events: int = 1 << 18, units: int = UNITS_CM) -> "Ingest":
+        """Open a streaming ingest (fd2_ingest_begin): pushed events are
+        transported batch by batch while the caller goes on pushing."""
+        h = ctypes.c_void_p()
+        self._check(self._lib.fd2_ingest_begin(self._h, int(batch_events), int(units), ctypes.byref(h)),
+                    "ingest_begin")
+        return Ingest(self, h)
+
     # -- execution
     def run(self):
         self._check(self._lib.fd2_run(self._h), "run")
@@ -325,3 +333,56 @@ class OpticalTransport:
             return None
         return {"fate": fate[:total_photons], "pix": pix[:2 * total_photons].reshape(-1, 2),
                 "seeds": seeds[:2 * total_photons].reshape(-1, 2), "steps": steps[:total_photons]}
+
+
+class Ingest:
+    """An open event stream of an OpticalTransport (include/fd2.h,
+    fd2_ingest_*).  The tallies after end() equal one submission and run of
+    the concatenated stream."""
+
+    def __init__(self, transport: OpticalTransport, handle):
+        self._t = transport
+        self._h = handle
+
+    def _check(self, st, where):
+        if st == 0:
+            return
+        try:
+            self._t._check(st, where)
+        finally:  # the stream is unusable after an error: release it
+            h, self._h = self._h, None
+            if h:
+                self._t._lib.fd2_ingest_end(h, None)
+
+    def push(self, x_cm, y_cm, z_cm, de_ev, hist):
+        """Events in the reference's units (cm, eV, 1-based history)."""
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x_cm, y_cm, z_cm, de_ev)]
+        h = np.ascontiguousarray(hist, dtype=np.int32)
+        self._check(self._t._lib.fd2_ingest_push(self._h, *[ptr(v) for v in a], ptr(h), len(h)), "ingest_push")
+
+    def push_um(self, x_um, y_um, z_um, e_ev, hist):
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (x_um, y_um, z_um, e_ev)]
+        h = np.ascontiguousarray(hist, dtype=np.int32)
+        self._check(self._t._lib.fd2_ingest_push_um(self._h, *[ptr(v) for v in a], ptr(h), len(h)), "ingest_push_um")
+
+    def push_file(self, path: str):
+        self._check(self._t._lib.fd2_ingest_file(self._h, path.encode()), "ingest_file")
+
+    def end(self) -> dict:
+        st = IngestStats()
+        h, self._h = self._h, None
+        if h is None:
+            raise Fd2Error(7, "ingest_end", "the stream is closed")
+        self._t._check(self._t._lib.fd2_ingest_end(h, ctypes.byref(st)), "ingest_end")
+        return st.as_dict()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        if self._h is not None:
+            if exc[0] is None:
+                self.end()
+            else:
+                h, self._h = self._h, None
+                self._t._lib.fd2_ingest_end(h, None)

@@ -287,6 +287,47 @@ FD2_API fd2_status fd2_write_events_text(const char *path, const fd2_events *ev)
 FD2_API fd2_status fd2_read_events_binary(const char *path, fd2_events *out);
 FD2_API fd2_status fd2_write_events_binary(const char *path, const fd2_events *ev);
 
+/* Streaming event ingest: the EDE tally's fill-and-flush loop
+ * (main/hybridMANTIS_tallyEnergyDepositionEvents.f:171-310, one blocking
+ * gpuoptical_ call per full buffer, main/hybridMANTIS_cuda_ver1_0.cu:107)
+ * without the block.  Pushed events fill one of two pinned staging batches
+ * of batch_events; a full batch is copied to the GPU on a copy stream and
+ * transported while the caller fills the other one, and a push waits only
+ * when both batches are still in flight.  Event indices run on across
+ * batches and the whole stream shares one run counter, so the tallies equal
+ * those of one fd2_submit_events (or _um) + fd2_run over the concatenated
+ * stream, bit for bit, for every batch size.  The PHS is built once, at
+ * fd2_ingest_end, from the per-history counts of the whole stream, so a
+ * history split across batches is one PHS entry.  Single-geometry
+ * contexts.  Between begin and end the context takes no submit, run,
+ * reset, autotune or replay (FD2_ERR_STATE); getters see partial tallies.
+ * Bad events and oversized photon counts are reported by fd2_ingest_end.
+ * units: FD2_UNITS_CM (x, y, z in cm and deposited energy in eV as doubles,
+ * the tally's buffer) or FD2_UNITS_UM (floats in um and eV). */
+typedef struct fd2_ingest fd2_ingest;
+enum { FD2_UNITS_CM = 0, FD2_UNITS_UM = 1 };
+typedef struct fd2_ingest_stats {
+    int64_t events;          /* events transported                         */
+    int64_t batches;         /* batches launched                           */
+    int64_t photons;         /* optical photons transported                */
+    double host_seconds;     /* fd2_ingest_begin to the end of fd2_ingest_end */
+    double push_wait_seconds;/* time pushes waited for a free staging batch */
+    float device_ms;         /* first copy to the PHS pass, CUDA events    */
+} fd2_ingest_stats;
+FD2_API fd2_status fd2_ingest_begin(fd2_ctx *ctx, int64_t batch_events, int32_t units, fd2_ingest **out);
+FD2_API fd2_status fd2_ingest_push(fd2_ingest *in, const double *x_cm, const double *y_cm, const double *z_cm,
+                                   const double *de_ev, const int32_t *hist, int64_t n);
+FD2_API fd2_status fd2_ingest_push_um(fd2_ingest *in, const float *x_um, const float *y_um, const float *z_um,
+                                      const float *e_ev, const int32_t *hist, int64_t n);
+/* Stream an EDE file through the ingest, reading it in batch-sized pieces:
+ * text rows "x y z de hist" (cm, eV, 1-based; '#' lines skipped) into a
+ * FD2_UNITS_CM ingest, or the binary form of fd2_write_events_binary
+ * (without geometry ids) into a FD2_UNITS_UM ingest. */
+FD2_API fd2_status fd2_ingest_file(fd2_ingest *in, const char *path);
+/* Transport what is left, build the PHS, wait, report the stream's status;
+ * releases `in` whatever the result.  stats may be NULL. */
+FD2_API fd2_status fd2_ingest_end(fd2_ingest *in, fd2_ingest_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -188,3 +188,65 @@ def test_invalid_arguments_are_rejected():
     g.pixel = 0
     assert lib.fd2_prf_dims(ctypes.byref(g), ctypes.byref(x), ctypes.byref(y)) == 1
     assert lib.fd2_parse_input_file(None, None) == 1
+
+
+def test_streaming_text_reader_edge_cases(tmp_path):
+    """The text reader streams the file through a 4 MiB window: rows that
+    straddle window ends, Fortran 'D' exponents, tabs and CR-LF endings, a
+    last row without a newline, extra columns (ignored) and malformed rows."""
+    rng = np.random.default_rng(3)
+    n = 120_000  # about 9 MB of text: the window slides twice
+    x, y, z = rng.uniform(0, 0.1, (3, n))
+    e = rng.uniform(1.0, 3.0e4, n)
+    h = np.sort(rng.integers(1, 5000, n)).astype(np.int32)
+    rows = []
+    for i in range(n):
+        s = f" {x[i]:16.9E} {y[i]:16.9E} {z[i]:16.9E} {e[i]:12.4E}{h[i]:8d}"
+        if i % 7 == 0:
+            s = s.replace("E", "D")
+        if i % 11 == 0:
+            s = s.replace(" ", "\t", 2)
+        if i % 13 == 0:
+            s += "  extra"
+        rows.append(s + ("\r\n" if i % 5 == 0 else "\n"))
+        if i % 1000 == 0:
+            rows.append("#  Past hist = 1\n\n")
+    text = "".join(rows).rstrip("\n")  # last row without its newline
+    (tmp_path / "big.txt").write_text(text)
+    es = hb.read_events_text(str(tmp_path / "big.txt"))
+    assert es.n == n
+    assert np.array_equal(es.hist, h)
+    # the reader's conversion: float(x_cm * (double)10000.0f) of the parsed value
+    xp = np.array([float(r.split()[0].replace("D", "E")) for r in rows if not r.startswith(("#", "\n"))])
+    assert np.array_equal(es.x_um, (xp * np.float64(np.float32(10000.0))).astype(np.float32))
+    for bad in ("1.0 2.0 3.0 4.0\n", "1.0 2.0 3.0 4.0 x\n", "1.0 2.0 zz 4.0 5\n", "1 2 3 4 99999999999\n"):
+        (tmp_path / "bad.txt").write_text(" 1.0 2.0 3.0 4.0 1\n" + bad)
+        with pytest.raises(hb.Fd2Error) as err:
+            hb.read_events_text(str(tmp_path / "bad.txt"))
+        assert err.value.status == 3  # FD2_ERR_PARSE
+
+
+def test_streaming_binary_reader_pieces(tmp_path):
+    """The binary reader reads each plane piece by piece (1 Mi events per
+    piece); a file larger than one piece and a truncated file."""
+    es = hb.synth_events(1, 500_000, 4)
+    assert es.n > (1 << 20)
+    hb.write_events_binary(str(tmp_path / "ev.bin"), es)
+    back = hb.read_events_binary(str(tmp_path / "ev.bin"))
+    for a in ("x_um", "y_um", "z_um", "e_ev", "hist"):
+        assert np.array_equal(getattr(es, a), getattr(back, a))
+    data = open(tmp_path / "ev.bin", "rb").read()
+    (tmp_path / "cut.bin").write_bytes(data[:-10])
+    with pytest.raises(hb.Fd2Error) as err:
+        hb.read_events_binary(str(tmp_path / "cut.bin"))
+    assert err.value.status == 3
+
+
+def test_ingest_entry_points_reject_null_handles():
+    lib = hb.load()
+    out = ctypes.c_void_p()
+    assert lib.fd2_ingest_begin(None, 1024, 0, ctypes.byref(out)) == 1
+    assert lib.fd2_ingest_push(None, None, None, None, None, None, 0) == 1
+    assert lib.fd2_ingest_push_um(None, None, None, None, None, None, 0) == 1
+    assert lib.fd2_ingest_file(None, b"x") == 1
+    assert lib.fd2_ingest_end(None, None) == 1
