@@ -149,6 +149,7 @@ EXPORTED = [
     "fd2_sg_train", "fd2_sg_set_lr", "fd2_sg_eval", "fd2_sg_num_params", "fd2_sg_get_params", "fd2_sg_set_params",
     "fd2_sg_get_hull", "fd2_sg_set_hull", "fd2_sg_save", "fd2_sg_load", "fd2_sg_loss_grad", "fd2_sg_predict",
     "fd2_sg_run",
+    "fd2_mtf", "fd2_nnps",
 ]
 
 
@@ -226,6 +227,11 @@ def load():
         "fd2_sg_loss_grad": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int32, P(ctypes.c_float), vp]),
         "fd2_sg_predict": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp]),
         "fd2_sg_run": (ctypes.c_int, [vp, vp, ctypes.c_double, P(SgStats)]),
+        "fd2_mtf": (ctypes.c_int, [ctypes.c_int32, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                   vp, vp, vp, vp]),
+        "fd2_nnps": (ctypes.c_int, [ctypes.c_int32, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                    ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.c_int32, vp, vp, vp, P(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

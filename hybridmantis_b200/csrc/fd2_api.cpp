@@ -207,6 +207,8 @@ fd2_status check_status(fd2_ctx *c)
     return FD2_OK;
 }
 
+void fit_window(fd2_ctx *c);
+
 void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *geom, int64_t n)
 {
     const DevGeom &g = c->dgeoms[0];
@@ -224,12 +226,11 @@ void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *g
         sy += y[i];
         ++k;
     }
-    c->cfg.window = (k > 0 && w >= 16) ? w : 0;
+    c->cfg.window = c->win_chosen = (k > 0 && w >= 16) ? w : 0;
     if (!c->cfg.window) return;
-    const int cx = (int)std::floor((sx / (double)k - g.lb_x) / g.pixel);
-    const int cy = (int)std::floor((sy / (double)k - g.lb_y) / g.pixel);
-    c->win_x0 = std::min(std::max(cx - w / 2, 0), g.xdim - w);
-    c->win_y0 = std::min(std::max(cy - w / 2, 0), g.ydim - w);
+    c->win_cx = (int)std::floor((sx / (double)k - g.lb_x) / g.pixel);
+    c->win_cy = (int)std::floor((sy / (double)k - g.lb_y) / g.pixel);
+    fit_window(c);
 }
 
 fd2::TransportArgs transport_args(fd2_ctx *c)
@@ -341,6 +342,24 @@ fd2_status build_graph(fd2_ctx *c)
     return FD2_OK;
 }
 
+// The shared-memory PRF window (a tally cache) picked at submission, shrunk
+// until ctas_per_sm CTAs of the configuration fit an SM's shared memory,
+// around the same centre.
+void fit_window(fd2_ctx *c)
+{
+    fd2::TransportConfig &k = c->cfg;
+    const int G = (int)c->geoms.size();
+    const size_t budget = 220 * 1024;
+    k.window = c->win_chosen;
+    while (k.window > 0 && fd2::transport_smem_bytes(k, G) * (size_t)k.ctas_per_sm > budget)
+        k.window = k.window > 16 ? k.window - 8 : 0;
+    if (k.window > 0) {
+        const DevGeom &g = c->dgeoms[0];
+        c->win_x0 = std::min(std::max(c->win_cx - k.window / 2, 0), g.xdim - k.window);
+        c->win_y0 = std::min(std::max(c->win_cy - k.window / 2, 0), g.ydim - k.window);
+    }
+}
+
 fd2_status set_config(fd2_ctx *c, const fd2::TransportConfig &cfg)
 {
     fd2::TransportConfig k = cfg;
@@ -349,9 +368,8 @@ fd2_status set_config(fd2_ctx *c, const fd2::TransportConfig &cfg)
     k.chunk = std::min(std::max(k.chunk, 1), 4096);
     k.refill = std::min(std::max(k.refill, 1), 32);
     k.fresnel = std::min(std::max(k.fresnel, 1), 32);
-    const int window = c->cfg.window;
     c->cfg = k;
-    c->cfg.window = window;
+    fit_window(c);
     FD2_CUDA(c, fd2::prepare_transport(c->cfg, (int)c->geoms.size()));
     c->graph_valid = false;
     return FD2_OK;
@@ -577,10 +595,11 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     c->geoms.assign(1, g);
     if ((st = alloc_tallies(c)) != FD2_OK) return bail(st);
     fd2::TransportConfig cfg;
-    cfg.block = c->opt.block_size > 0 ? c->opt.block_size : 256;
+    // defaults: what the autotuner picks for the config-1 workload on a B200
+    cfg.block = c->opt.block_size > 0 ? c->opt.block_size : (c->opt.radial_bins > 0 ? 256 : 320);  // label mode: 256
     cfg.ctas_per_sm = c->opt.ctas_per_sm > 0 ? c->opt.ctas_per_sm : 2;
     cfg.chunk = c->opt.chunk > 0 ? c->opt.chunk : 32;
-    cfg.refill = c->opt.refill > 0 ? c->opt.refill : 8;
+    cfg.refill = c->opt.refill > 0 ? c->opt.refill : 4;
     cfg.fresnel = c->opt.fresnel_batch > 0 ? c->opt.fresnel_batch : 8;
     if ((st = set_config(c, cfg)) != FD2_OK) return bail(st);
     *out = c;
@@ -1111,7 +1130,7 @@ fd2_status fd2_autotune(fd2_ctx *c, int32_t budget_runs)
     float best_ms = 0.0f;
     if ((st = time_cfg(best, &best_ms)) != FD2_OK) return st;
     int runs = 2;
-    const std::vector<int> blocks = {128, 256, 384, 512};
+    const std::vector<int> blocks = {128, 256, 320, 384, 512};
     const std::vector<int> ctas = {1, 2, 3, 4};
     const std::vector<int> chunks = {8, 16, 32, 64, 128};
     const std::vector<int> refills = {1, 4, 8, 16};
@@ -1130,8 +1149,11 @@ fd2_status fd2_autotune(fd2_ctx *c, int32_t budget_runs)
                                         : k.fresnel;
                 if (slot == v) continue;
                 slot = v;
-                // the CTA's shared memory must fit ctas_per_sm times
-                if (fd2::transport_smem_bytes(k, (int)c->geoms.size()) * (size_t)k.ctas_per_sm > 220 * 1024) continue;
+                // the CTA's shared memory must fit ctas_per_sm times (set_config
+                // shrinks the PRF window to fit; without it, skip)
+                fd2::TransportConfig bare = k;
+                bare.window = 0;
+                if (fd2::transport_smem_bytes(bare, (int)c->geoms.size()) * (size_t)k.ctas_per_sm > 220 * 1024) continue;
                 float ms = 0.0f;
                 if (time_cfg(k, &ms) != FD2_OK) continue;
                 runs += 2;

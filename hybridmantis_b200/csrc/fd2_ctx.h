@@ -71,6 +71,7 @@ struct fd2_ctx {
     fd2_ingest *ingest = nullptr; // the open ingest, ended by fd2_destroy
     fd2::TransportConfig cfg;
     int win_x0 = 0, win_y0 = 0;
+    int win_chosen = 0, win_cx = 0, win_cy = 0;  // window and centre picked at submission
     int64_t last_photons = 0;
 
     // float-libm corrections of the reference-arithmetic replay

@@ -157,6 +157,7 @@ struct Walker {
     float xc, yc;       // centre of the current column
     float ex, ey, ez;   // emission point (the event)
     float dist;         // path length
+    float budget;       // absorption lengths left before bulk absorption
     uint32_t rebound;   // boundary interactions
     int ii, jj;         // detection pixel (-1: outside the PRF bounds)
     // Philox stream of the photon and the lane's uniform ring.  At the start
@@ -219,6 +220,7 @@ struct Walker {
         ii = -1; jj = -1;
         top_up();
         emit(first);
+        budget = -__logf(u());  // Exp(1)
     }
 
     // Isotropic emission; the first photon of an event rejects |cos| <= 0.01
@@ -322,8 +324,13 @@ struct Walker {
         if (outside_detector(g)) return kLost;
         dist += d;
         if (g.neg_inv_mu != 0.0f) {
-            const float dabs = g.neg_inv_mu * __logf(u());
-            if (d >= dabs && d >= 0.0f) return kAbsBulk;
+            // bulk absorption: one Exp(1) budget of absorption lengths per
+            // photon, spent flight by flight; by the exponential's lack of
+            // memory the same law as the reference's fresh draw per flight
+            // (absorbed when d >= -ln(u) / mu)
+            const float da = d * g.mu;
+            if (da >= budget && d >= 0.0f) return kAbsBulk;
+            budget -= da;
         }
         return kAlive;
     }

@@ -670,9 +670,12 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
 }
 
 // Register budgets: blocks of up to 256 threads are compiled for 2, 3 or 4
-// resident CTAs per SM (128, 85, 64 registers); larger blocks for one.
+// resident CTAs per SM (128, 85, 64 registers), blocks of 320 threads for
+// two (102 registers: 20 warps per SM; the walk fits without spills, 352
+// threads would spill), other larger blocks for one.
 #define FD2_TRANSPORT_VARIANTS(X)                          \
     X(false, 512, 1, false) X(false, 256, 2, false)        \
+    X(false, 320, 2, false) X(true, 320, 2, false)         \
     X(false, 256, 3, false) X(false, 256, 4, false)        \
     X(true, 512, 1, false) X(true, 256, 2, false)          \
     X(true, 256, 3, false) X(true, 256, 2, true)
@@ -719,12 +722,14 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
         if (cfg.block > 256) return cudaErrorInvalidConfiguration;
         transport_kernel<true, 256, 2, true><<<(unsigned)(sm_count * 2), cfg.block, smem, s>>>(a);
     } else if (!multi) {
-        if (per_sm == 1) transport_kernel<false, 512, 1><<<grid, cfg.block, smem, s>>>(a);
+        if (cfg.block == 320) transport_kernel<false, 320, 2><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 1) transport_kernel<false, 512, 1><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 2) transport_kernel<false, 256, 2><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 3) transport_kernel<false, 256, 3><<<grid, cfg.block, smem, s>>>(a);
         else transport_kernel<false, 256, 4><<<grid, cfg.block, smem, s>>>(a);
     } else {
-        if (per_sm == 1) transport_kernel<true, 512, 1><<<grid, cfg.block, smem, s>>>(a);
+        if (cfg.block == 320) transport_kernel<true, 320, 2><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 1) transport_kernel<true, 512, 1><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 2) transport_kernel<true, 256, 2><<<grid, cfg.block, smem, s>>>(a);
         else transport_kernel<true, 256, 3><<<grid, cfg.block, smem, s>>>(a);
     }
