@@ -84,6 +84,12 @@ struct fd2_sg {
 
     // event-pipeline buffers (fd2_sg_run)
     struct RunBuffers *run = nullptr;
+
+    // forward GEMMs on tcgen05 (fd2_sg_tc.cuh) unless FD2_SG_GEMM=mma; a
+    // tile whose completion wait gave up sets the fault word
+    bool use_tc = true;
+    unsigned *d_tc_fault = nullptr;
+    int sm_count = 148;
 };
 
 fd2_status sg_fail(fd2_sg *s, fd2_status st, const std::string &msg);
@@ -91,3 +97,6 @@ fd2_status sg_cuda(fd2_sg *s, cudaError_t e, const char *what);
 cudaError_t sg_forward(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *x0, int rows, const int *m_limit,
                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, __nv_bfloat16 *h3, float *out);
 void sg_free_run_buffers(fd2_sg *s);
+// FD2_ERR_DEVICE_ABORT (and the fault word cleared) when a tensor-core tile
+// gave up waiting since the last check; call after a stream synchronisation.
+fd2_status sg_tc_check(fd2_sg *s);

@@ -476,6 +476,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
     if (e == cudaSuccess) e = cudaMemcpyAsync(stat, R->d_stat, sizeof stat, cudaMemcpyDeviceToHost, q);
     if (e == cudaSuccess) e = cudaStreamSynchronize(q);
     if (e != cudaSuccess) return sg_cuda(s, e, "surrogate run");
+    if ((st = sg_tc_check(s)) != FD2_OK) return st;
     c->counts_ready = true;
     c->ran_once = true;
     c->graph_valid = false;  // the counts were rewritten outside the graph

@@ -1,0 +1,244 @@
+// fd2_sg_tc.cuh -- the surrogate's forward GEMMs on the 5th-generation tensor
+// cores: tcgen05.mma with the accumulator in tensor memory (TMEM).
+//
+// C[M x N] = A[M x K] B[N x K]^T (both operands K-contiguous, BF16), FP32
+// accumulation, epilogue bias + ReLU to BF16 or bias to FP32 -- the four
+// forward products of the MLP (kc x kc in fd2_sg_gemm.cuh).  Persistent CTAs
+// of four warps (at most one per SM) walk the 128-row tiles, the whole
+// contraction of a tile in one pass:
+//   1. the CTA stages all of B (N x K) once and, per tile, its A tile
+//      (128 x K) in shared memory (cp.async, all copies in flight together)
+//      in the canonical
+//      no-swizzle K-major layout of the UMMA descriptors: 8-row x 16-byte
+//      core matrices, 128 bytes each, the 8-row groups of one 16-byte K
+//      chunk contiguous (stride 128 B, the descriptor's SBO) and successive
+//      K chunks `rows x 16` bytes apart (its LBO);
+//   2. warp 0 allocates N (rounded up to a power of two >= 32) TMEM columns
+//      once for the CTA;
+//   3. one thread issues K/16 tcgen05.mma.cta_group::1.kind::f16 (M = 128,
+//      N, K = 16 each), advancing both descriptors' start addresses by two
+//      K chunks per instruction, and commits them to an mbarrier;
+//   4. every warp waits on the mbarrier (bounded; one phase per tile), reads
+//      its 32 TMEM lanes (rows) with tcgen05.ld 32x32b.x16 and applies the
+//      epilogue;
+//   5. after the last tile warp 0 frees the TMEM columns.
+// Bit layouts of the shared-memory and instruction descriptors follow the
+// PTX ISA's tcgen05 matrix-descriptor and instruction-descriptor formats for
+// kind::f16 (as CUTLASS's cute/arch/mma_sm100_desc.hpp spells them out).
+// Requirements: K % 16 == 0, K <= 256; N % 16 == 0, 16 <= N <= 256; row
+// strides multiples of 8 elements.  Rows past M or past *m_limit are
+// zero-filled and not stored.  No TMA and no multicast: operands are staged
+// with 16-byte cp.async copies from this GPU's memory.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "fd2_sg_gemm.cuh"
+
+namespace fd2 {
+namespace sg {
+
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 128;
+constexpr int kTcMaxK = 256, kTcMaxN = 256;
+// bounded waits: the MMAs of one tile take microseconds
+constexpr long long kTcWaitSpins = 1LL << 22;
+
+struct TcArgs {
+    const __nv_bfloat16 *A;
+    const __nv_bfloat16 *B;
+    int lda, ldb, M, N, K;
+    const int *m_limit;
+    int epi;  // kEpiBiasReluBf16 or kEpiBiasF32
+    const float *bias;
+    void *C;
+    int ldc;
+    unsigned *fault;  // set when a wait gives up (the tile is then not stored)
+};
+
+// Dynamic shared memory of one CTA: A tile + B.
+__host__ __device__ inline size_t tc_smem_bytes(int N, int K)
+{
+    return (size_t)(kTcRows + N) * (size_t)K * sizeof(__nv_bfloat16);
+}
+
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);              // start address, 16-byte units, bits [0,14)
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;   // leading-dimension byte offset, bits [16,30)
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;   // stride-dimension byte offset, bits [32,46)
+    d |= (uint64_t)1 << 46;                              // descriptor version for sm_100, bits [46,48)
+    // base offset 0, legacy LBO mode, layout type 0 = no swizzle (bits [61,64))
+    return d;
+}
+
+__host__ __device__ constexpr uint32_t tc_instr_desc(int M, int N)
+{
+    return (1u << 4)                      // D format: F32
+           | (1u << 7)                    // A format: BF16
+           | (1u << 10)                   // B format: BF16
+           | ((uint32_t)(N >> 3) << 17)   // N / 8
+           | ((uint32_t)(M >> 4) << 24);  // M / 16; A and B K-major (bits 15, 16 = 0)
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity)
+{
+    for (long long i = 0; i < kTcWaitSpins; ++i) {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// Stage rows [0, rows) of a K-contiguous matrix (row stride ld) into the
+// canonical layout at `dst` with asynchronous 16-byte copies (all of a
+// thread's copies in flight at once); rows >= valid are zero-filled (a copy
+// of 0 source bytes).  Consecutive threads take 8 rows of one K chunk (128
+// contiguous bytes of shared memory), then the next chunks of the same rows.
+__device__ __forceinline__ void tc_stage(unsigned char *dst, const __nv_bfloat16 *src, int ld, int rows, int valid,
+                                         int K)
+{
+    const int kc = K / 8;  // 16-byte chunks per row
+    const int total = rows * kc;
+    for (int L = threadIdx.x; L < total; L += blockDim.x) {
+        const int ri = L & 7, t = L >> 3;
+        const int c = t % kc, rg = t / kc;
+        const int r = rg * 8 + ri;
+        const bool ok = r < valid;
+        const __nv_bfloat16 *g = src + (long long)(ok ? r : 0) * ld + c * 8;
+        const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst + (size_t)c * rows * 16 + (size_t)rg * 128 +
+                                                              (size_t)ri * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(g), "r"(ok ? 16 : 0) : "memory");
+    }
+}
+
+template <int kEpi>
+__global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long s_mbar;
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_ok;
+
+    int M = g.M;
+    if (g.m_limit) M = min(M, *g.m_limit);
+    const int ntiles = (M + kTcRows - 1) / kTcRows;
+    if ((int)blockIdx.x >= ntiles) return;  // whole CTA, before any TMEM or barrier use
+    const int N = g.N, K = g.K;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *sA = tc_smem;
+    unsigned char *sB = tc_smem + (size_t)kTcRows * K * 2;
+    const uint32_t cols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+
+    // TMEM columns (warp 0) and the completion barrier (thread 0), once
+    if (warp == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_taddr);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        s_ok = 1;
+    }
+    // B stays resident for all of the CTA's tiles
+    tc_stage(sB, g.B, g.ldb, N, N, K);
+    const uint32_t idesc = tc_instr_desc(kTcRows, N);
+    const uint32_t lbo_a = kTcRows * 16, lbo_b = (uint32_t)N * 16;
+    uint32_t taddr = 0;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int m0 = tile * kTcRows;
+        const int valid = min(kTcRows, M - m0);
+        tc_stage(sA, g.A + (long long)m0 * g.lda, g.lda, kTcRows, valid, K);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        // the staged operands become visible to the tensor core's (async)
+        // proxy; the previous tile's TMEM reads are ordered before the MMAs
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        taddr = s_taddr;
+        if (threadIdx.x == 0) {
+            const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sA);
+            const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
+            for (int s = 0; s < K / 16; ++s) {
+                // K step s: 16-byte K chunks 2s and 2s+1
+                const uint64_t da = tc_smem_desc(a0 + 2u * s * lbo_a, lbo_a, 128);
+                const uint64_t db = tc_smem_desc(b0 + 2u * s * lbo_b, lbo_b, 128);
+                const uint32_t acc = s > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                    :
+                    : "r"(taddr), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                         : "memory");
+        }
+        __syncwarp();
+        // the barrier completes one phase per tile
+        if (!tc_wait(mbar, (uint32_t)(it & 1))) {
+            s_ok = 0;
+            if (g.fault) atomicOr(g.fault, 1u);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (!s_ok) {
+            // the MMAs may still be running: give them another bounded wait
+            // before their accumulator columns are freed
+            tc_wait(mbar, (uint32_t)(it & 1));
+            break;
+        }
+        // epilogue: warp w owns TMEM lanes (tile rows) 32w .. 32w + 31
+        const int r = warp * 32 + lane;
+        const long long row = (long long)m0 + r;
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t src = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(src));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (r < valid) {
+                float f[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) f[j] = __uint_as_float(v[j]) + g.bias[c0 + j];
+                if (kEpi == kEpiBiasReluBf16) {
+                    __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(fmaxf(f[j], 0.0f));
+                    uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) + row * g.ldc + c0);
+                    dst[0] = reinterpret_cast<const uint4 *>(o)[0];
+                    dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+                } else {
+                    float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(g.C) + row * g.ldc + c0);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dst[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols));
+}
+
+}  // namespace sg
+}  // namespace fd2

@@ -23,12 +23,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "fd2.h"
 #include "fd2_sg_gemm.cuh"
+#include "fd2_sg_tc.cuh"
 #include "fd2_sg_internal.h"
 #include "fd2_sg_mix.cuh"
 #include "fd2_surrogate.h"
@@ -351,6 +353,45 @@ GemmArgs gemm_args(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int 
 
 }  // namespace
 
+// One forward product (K-contiguous operands, bias epilogue): tcgen05 when
+// the shapes fit one pass of fd2_sg_tc.cuh, else the mma.sync kernel.
+static cudaError_t sg_dense(fd2_sg *s, cudaStream_t st, const GemmArgs &g)
+{
+    const bool tc = s->use_tc && g.K % 16 == 0 && g.K <= kTcMaxK && g.N % 16 == 0 && g.N >= 16 && g.N <= kTcMaxN &&
+                    g.lda % 8 == 0 && g.ldb % 8 == 0 && g.ldc % 16 == 0 && g.M > 0;
+    if (!tc) return sg_gemm(st, true, true, g, 1);
+    TcArgs t;
+    t.A = g.A;
+    t.B = g.B;
+    t.lda = g.lda;
+    t.ldb = g.ldb;
+    t.M = g.M;
+    t.N = g.N;
+    t.K = g.K;
+    t.m_limit = g.m_limit;
+    t.epi = g.epi;
+    t.bias = g.bias;
+    t.C = g.C;
+    t.ldc = g.ldc;
+    t.fault = s->d_tc_fault;
+    const unsigned grid = (unsigned)std::min((g.M + kTcRows - 1) / kTcRows, s->sm_count);
+    const size_t smem = tc_smem_bytes(g.N, g.K);
+    if (g.epi == kEpiBiasReluBf16) gemm_tc_kernel<kEpiBiasReluBf16><<<grid, kTcThreads, smem, st>>>(t);
+    else if (g.epi == kEpiBiasF32) gemm_tc_kernel<kEpiBiasF32><<<grid, kTcThreads, smem, st>>>(t);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+fd2_status sg_tc_check(fd2_sg *s)
+{
+    if (!s || !s->d_tc_fault) return FD2_OK;
+    unsigned f = 0;
+    SG_CUDA(s, cudaMemcpy(&f, s->d_tc_fault, sizeof f, cudaMemcpyDeviceToHost));
+    if (!f) return FD2_OK;
+    SG_CUDA(s, cudaMemset(s->d_tc_fault, 0, sizeof f));
+    return sg_fail(s, FD2_ERR_DEVICE_ABORT, "a tensor-core GEMM tile gave up waiting for its MMAs");
+}
+
 // Forward pass over `rows` input rows in sg->x0 (row capacity >= rows):
 // activations h1..h3 (BF16) and out (FP32 [rows][64]).
 cudaError_t sg_forward(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *x0, int rows, const int *m_limit,
@@ -361,19 +402,19 @@ cudaError_t sg_forward(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *x0, int 
     GemmArgs g = gemm_args(x0, kInPad, s->pb + s->off[kW1], kInPad, rows, H, kInPad, kEpiBiasReluBf16, h1, H);
     g.bias = s->p + s->off[kB1];
     g.m_limit = m_limit;
-    if ((e = sg_gemm(st, true, true, g, 1)) != cudaSuccess) return e;
+    if ((e = sg_dense(s, st, g)) != cudaSuccess) return e;
     g = gemm_args(h1, H, s->pb + s->off[kW2], H, rows, H, H, kEpiBiasReluBf16, h2, H);
     g.bias = s->p + s->off[kB2];
     g.m_limit = m_limit;
-    if ((e = sg_gemm(st, true, true, g, 1)) != cudaSuccess) return e;
+    if ((e = sg_dense(s, st, g)) != cudaSuccess) return e;
     g = gemm_args(h2, H, s->pb + s->off[kW3], H, rows, H, H, kEpiBiasReluBf16, h3, H);
     g.bias = s->p + s->off[kB3];
     g.m_limit = m_limit;
-    if ((e = sg_gemm(st, true, true, g, 1)) != cudaSuccess) return e;
+    if ((e = sg_dense(s, st, g)) != cudaSuccess) return e;
     g = gemm_args(h3, H, s->pb + s->off[kW4], H, rows, kOutPad, H, kEpiBiasF32, out, kOutPad);
     g.bias = s->p + s->off[kB4];
     g.m_limit = m_limit;
-    return sg_gemm(st, true, true, g, 1);
+    return sg_dense(s, st, g);
 }
 
 namespace {
@@ -637,6 +678,22 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
         alloc(&s->ws, (size_t)kMaxSplits * std::max<size_t>((size_t)s->hidden * s->hidden, (size_t)kOutPad * s->hidden)))
         return bail(FD2_ERR_OUT_OF_MEMORY);
     if (cudaMemcpy(s->d_lr, &s->lr, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return bail(FD2_ERR_CUDA);
+    if (alloc(&s->d_tc_fault, 1) || cudaMemset(s->d_tc_fault, 0, sizeof(unsigned)) != cudaSuccess)
+        return bail(FD2_ERR_OUT_OF_MEMORY);
+    {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) == cudaSuccess && sms > 0)
+            s->sm_count = sms;
+        const char *env = std::getenv("FD2_SG_GEMM");
+        s->use_tc = !(env && std::strcmp(env, "mma") == 0);
+        // the tcgen05 kernels' shared memory (outside any stream capture)
+        const int bytes = (int)tc_smem_bytes(kTcMaxN, kTcMaxK);
+        if (cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasReluBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+                cudaSuccess)
+            return bail(FD2_ERR_CUDA);
+    }
     const std::vector<uint8_t> live = live_mask(s);
     if (cudaMemcpy(s->d_live, live.data(), P, cudaMemcpyHostToDevice) != cudaSuccess) return bail(FD2_ERR_CUDA);
     if (cudaMemset(s->g, 0, sizeof(float) * P) != cudaSuccess) return bail(FD2_ERR_CUDA);
@@ -685,7 +742,7 @@ void fd2_sg_destroy(fd2_sg *s)
                     (void *)s->d_step, (void *)s->d_acc, (void *)s->d_lr, (void *)s->ws, (void *)s->x0, (void *)s->h1, (void *)s->h2,
                     (void *)s->h3, (void *)s->d1, (void *)s->d2, (void *)s->d3, (void *)s->out, (void *)s->dout,
                     (void *)s->target, (void *)s->has_rad, (void *)s->ylab, (void *)s->d_feat, (void *)s->d_photons,
-                    (void *)s->d_detected, (void *)s->d_radial})
+                    (void *)s->d_detected, (void *)s->d_radial, (void *)s->d_tc_fault})
         if (p) cudaFree(p);
     sg_free_run_buffers(s);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -815,6 +872,7 @@ fd2_status fd2_sg_eval(fd2_sg *s, float *loss, float *det_loss, float *radial_lo
     double acc[4];
     SG_CUDA(s, cudaMemcpyAsync(acc, s->d_acc, sizeof acc, cudaMemcpyDeviceToHost, s->stream));
     SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    if ((st = sg_tc_check(s)) != FD2_OK) return st;
     if (loss) *loss = (float)(acc[0] / (double)count);
     if (det_loss) *det_loss = (float)(acc[1] / (double)count);
     if (radial_loss) *radial_loss = (float)(acc[2] / (double)count);
@@ -850,6 +908,7 @@ fd2_status fd2_sg_train(fd2_sg *s, int32_t steps, float *train_loss, float *val_
     double acc[4] = {0, 0, 0, 0};
     SG_CUDA(s, cudaMemcpyAsync(acc, s->d_acc, sizeof acc, cudaMemcpyDeviceToHost, s->stream));
     SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    if ((st = sg_tc_check(s)) != FD2_OK) return st;
     if (train_loss) *train_loss = tail > 0 ? (float)(acc[0] / ((double)tail * s->batch)) : 0.0f;
     if (val_loss) {
         st = fd2_sg_eval(s, val_loss, nullptr, nullptr);
@@ -901,6 +960,7 @@ fd2_status fd2_sg_loss_grad(fd2_sg *s, const float *features, const int32_t *pho
     cudaFree(dd);
     cudaFree(dr);
     SG_CUDA(s, e);
+    if (fd2_status t = sg_tc_check(s)) return t;
     if (loss) *loss = (float)(acc[0] / b);
     if (grad) for_each_public(s, [&](int64_t k, int64_t i) { grad[k] = g[(size_t)i]; });
     return FD2_OK;
@@ -933,7 +993,7 @@ fd2_status fd2_sg_predict(fd2_sg *s, const float *features, int64_t n, float *ou
     }
     cudaFree(df);
     SG_CUDA(s, e);
-    return FD2_OK;
+    return sg_tc_check(s);
 }
 
 // File: "FD2SG002", hidden, bins, radial_max, normalisation box, routing

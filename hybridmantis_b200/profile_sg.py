@@ -1,0 +1,40 @@
+"""Surrogate forward pass for profilers (ncu): ``python -m hybridmantis_b200.profile_sg``.
+
+Runs the network's forward pass (fd2_sg_predict: input normalisation and the
+four GEMMs) on ``--rows`` seeded random inputs ``--runs`` times, with random
+weights of the full-size network, and prints the host time per pass.  With
+FD2_SG_GEMM=mma in the environment the GEMMs run on the mma.sync kernel
+instead of tcgen05.
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import surrogate as sgm
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rows", type=int, default=65536)
+    ap.add_argument("--runs", type=int, default=6)
+    ap.add_argument("--hidden", type=int, default=256)
+    a = ap.parse_args()
+    rng = np.random.default_rng(1)
+    with sgm.Surrogate(hidden=a.hidden, batch=a.rows) as s:
+        s.set_params(rng.normal(0, 0.05, s.num_params()).astype(np.float32))
+        s.set_hull(np.zeros(8, np.float32), np.ones(8, np.float32))
+        f = rng.uniform(0, 1, (a.rows, 8)).astype(np.float32)
+        ms = []
+        for _ in range(a.runs):
+            t0 = time.perf_counter()
+            out = s.predict(f)
+            ms.append((time.perf_counter() - t0) * 1e3)
+    print(json.dumps({"gemm": os.environ.get("FD2_SG_GEMM", "tc"), "rows": a.rows, "predict_ms": ms,
+                      "mean_abs_output": float(np.abs(out).mean())}))
+
+
+if __name__ == "__main__":
+    main()

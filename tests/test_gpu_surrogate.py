@@ -135,3 +135,29 @@ def test_contexts_with_different_shared_memory_alternate(require_gpu):
         sgm.label_points(geoms, 16, 500, seed=3)
         t.run_sync()
         assert t.counters()["generated"] > first
+
+
+def test_tensor_core_forward_matches_mma_sync(require_gpu, monkeypatch):
+    """The forward GEMMs run on tcgen05 (TMEM accumulators); the mma.sync
+    kernel (FD2_SG_GEMM=mma) computes the same BF16 x BF16 -> FP32 products
+    in another summation order.  Ragged batch (1,000 rows: 7 full 128-row
+    tiles and a partial one), full-size network."""
+    H = 256
+    p, f, lo, hi, ph, de, ra = _random_problem(5, 1000, H)
+    outs = []
+    for mode in ("tc", "mma"):
+        if mode == "mma":
+            monkeypatch.setenv("FD2_SG_GEMM", "mma")
+        else:
+            monkeypatch.delenv("FD2_SG_GEMM", raising=False)
+        with sgm.Surrogate(hidden=H, batch=512) as s:
+            s.set_params(p)
+            s.set_hull(lo, hi)
+            outs.append(s.predict(f))
+    a, b = outs
+    assert a.shape == (1000, 25) and np.all(np.isfinite(a))
+    scale = np.abs(b).max()
+    # BF16 hidden activations: a different FP32 summation order can move an
+    # activation by one BF16 step now and then
+    assert np.abs(a - b).max() <= 2e-2 * scale, np.abs(a - b).max()
+    assert np.abs(a - b).mean() <= 1e-3 * scale, np.abs(a - b).mean()
