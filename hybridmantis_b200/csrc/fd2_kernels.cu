@@ -461,6 +461,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         // Fresnel part for the parked lanes together once `fresnel_batch` of
         // them wait (or nothing else runs)
         int fate = kAlive;
+        if (alive) w.top_up();  // one warp-wide refill per round for every live lane
         if (alive && !parked) {
             if (!xretry) {
                 fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
@@ -484,7 +485,6 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             const unsigned busy = __ballot_sync(kFull, alive && !parked && fate == kAlive);
             if ((unsigned)__popc(waiting) >= fresnel_min || busy == 0) {
                 if (parked) {
-                    w.top_up();  // the parked lanes' rings, refilled together
                     fate = kMulti ? w.surface_fresnel(s_geom[geom]) : w.surface_fresnel(a.g0);
                     parked = false;
                 }
