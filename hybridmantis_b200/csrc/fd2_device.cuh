@@ -69,7 +69,7 @@ __device__ __forceinline__ float u01(uint32_t r)
 
 constexpr int kURing = 32;      // uniforms buffered per lane
 constexpr int kURingLow = 12;  // inside a step: a lane at or below this level must generate
-constexpr int kURingStep = 24; // at a round's start the warp generates while a lane is at or below this
+constexpr int kURingStep = 24; // the round's refill generates while a lane is at or below this
 
 // Internal step result: the photon waits at a column wall for the Fresnel
 // part of its surface interaction (not a fate).
@@ -131,7 +131,7 @@ struct RefillState {
     uint32_t tail, block;
 };
 
-// Refill inside a step: rarely taken once the round start leaves every ring
+// Refill inside a step: rarely taken once the round's refill leaves every ring
 // above kURingStep, so it is one out-of-line copy instead of an inlined
 // Philox at every loop of the walk (the walk's code then stays small enough
 // for the instruction cache).  Fills the lane's ring completely.
@@ -160,11 +160,12 @@ struct Walker {
     float budget;       // absorption lengths left before bulk absorption
     uint32_t rebound;   // boundary interactions
     int ii, jj;         // detection pixel (-1: outside the PRF bounds)
-    // Philox stream of the photon and the lane's uniform ring.  At the start
-    // of each round of the transport loop the warp tops the ring of every
-    // live lane up above kURingStep (top_up, one inlined copy for the whole
-    // round: steps, crosstalk attempts and parked lanes alike); at every
-    // loop iteration and new-normal attempt inside a step a ring at or below
+    // Philox stream of the photon and the lane's uniform ring.  Once per
+    // round of the transport loop, after the steps, the warp tops the ring of
+    // every lane whose photon goes on up above kURingStep (top_up, one
+    // inlined copy for the whole round: crosstalk attempts, parked lanes and
+    // the next step alike); at the start of a step and at every loop
+    // iteration and new-normal attempt inside one, a ring at or below
     // kURingLow is refilled out of line (top_up_inner).  No segment
     // between two checks draws more than 7, so a draw is a plain
     // shared-memory load.  `underflow` records a draw from an empty ring
@@ -678,6 +679,7 @@ struct Walker {
     template <class G>
     __device__ __forceinline__ int step(const G &g)
     {
+        top_up_inner();  // a step draws at most 6 uniforms; the round's refill follows it
         int f = flight(g);
         if (f != kAlive) return f;
         if (fabsf(pz + g.half) < kEps) {

@@ -461,19 +461,21 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         // Fresnel part for the parked lanes together once `fresnel_batch` of
         // them wait (or nothing else runs)
         int fate = kAlive;
-        if (alive) w.top_up();  // one warp-wide refill per round for every live lane
-        if (alive && !parked) {
-            if (!xretry) {
-                fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
-                if (fate == kNeedsFresnel) {
-                    parked = true;
-                    fate = kAlive;
-                }
+        if (alive && !parked && !xretry) {
+            fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
+            if (fate == kNeedsFresnel) {
+                parked = true;
+                fate = kAlive;
             }
+        }
+        // one warp-wide refill per round, in one inlined copy, for every lane
+        // whose photon goes on: crosstalk attempts, parked lanes and the next
+        // round's step alike
+        if ((alive && fate == kAlive) || fate == kNeedsNormal) w.top_up();
+        if (alive && !parked) {
             // crosstalk: one attempt at the next column's normal per round, so
             // a rejected attempt is retried beside the other lanes' first ones
             if (xretry || fate == kNeedsNormal) {
-                w.top_up();  // warp-wide refill for fresh and retried attempts alike
                 fate = kMulti ? w.crosstalk_normal(s_geom[geom], xtries) : w.crosstalk_normal(a.g0, xtries);
                 xretry = fate == kRetryNormal;
                 if (xretry) fate = kAlive;
