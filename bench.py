@@ -154,10 +154,10 @@ class CpuReference:
 
 
 # DRAM bytes per photon of the transport kernel: dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture (3,342,080 B for 4,690,971 photons
+# dram__bytes_write.sum of one ncu capture (3,338,240 B for 4,690,971 photons
 # of the config-1 stream, 2,000 x-rays); the traffic is one event record per
 # chunk and grows in proportion to the photons.
-TRANSPORT_DRAM_BYTES_PER_PHOTON = 3342080.0 / 4690971.0
+TRANSPORT_DRAM_BYTES_PER_PHOTON = 3338240.0 / 4690971.0
 
 
 def reference_gpu(es, nphot, device):
