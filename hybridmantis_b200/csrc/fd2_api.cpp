@@ -124,6 +124,8 @@ fd2_status alloc_tallies(fd2_ctx *c)
     int64_t off = 0;
     for (const auto &g : c->geoms) {
         DevGeom d = make_dev_geom(g);
+        d.grid = c->opt.column_grid;
+        d.pitch = (float)(2.0 * g.radius + c->opt.grid_gap_um);
         d.prf_offset = off;
         off += (int64_t)d.xdim * d.ydim;
         c->dgeoms.push_back(d);
@@ -534,6 +536,8 @@ void fd2_default_options(fd2_options *o)
     o->event_base = 0;
     o->radial_bins = 0;
     o->radial_max_um = 200.0;
+    o->column_grid = 0;
+    o->grid_gap_um = 0.5;
 }
 
 const char *fd2_last_error(const fd2_ctx *c) { return c ? c->last_error.c_str() : "no context"; }
@@ -551,7 +555,8 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     else fd2_default_options(&c->opt);
     if (c->opt.max_photons_per_event <= 0) c->opt.max_photons_per_event = 900000;
     if (c->opt.event_base < 0 || c->opt.radial_bins < 0 || c->opt.radial_bins > 4096 ||
-        (c->opt.radial_bins > 0 && !(c->opt.radial_max_um > 0.0))) {
+        (c->opt.radial_bins > 0 && !(c->opt.radial_max_um > 0.0)) || c->opt.column_grid < 0 ||
+        c->opt.column_grid > 1 || (c->opt.column_grid && (!(c->opt.grid_gap_um > 0.0) || c->opt.radial_bins > 0))) {
         delete c;
         return FD2_ERR_INVALID_ARGUMENT;
     }
@@ -653,6 +658,7 @@ fd2_status fd2_set_geometries(fd2_ctx *c, const fd2_geometry *g, int32_t n)
     if (!c || !g || n <= 0 || n > 256) return fail(c, FD2_ERR_INVALID_ARGUMENT, "1..256 geometries");
     for (int32_t i = 0; i < n; ++i)
         if (!valid_geometry(g[i])) return fail(c, FD2_ERR_INVALID_ARGUMENT, "invalid geometry " + std::to_string(i));
+    if (c->opt.column_grid && n > 1) return fail(c, FD2_ERR_STATE, "the column lattice is for one geometry");
     FD2_CUDA(c, cudaSetDevice(c->device));
     FD2_CUDA(c, cudaStreamSynchronize(c->stream));
     c->geoms.assign(g, g + n);
@@ -1042,6 +1048,7 @@ fd2_status fd2_replay(fd2_ctx *c, int32_t mode, int32_t seed_input, int64_t even
     if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c || (mode != FD2_REPLAY_REF && mode != FD2_REPLAY_FP64) || seed_input <= 0 || event_index_base < 0)
         return fail(c, FD2_ERR_INVALID_ARGUMENT, "replay mode / seed");
+    if (c->opt.column_grid) return fail(c, FD2_ERR_STATE, "the replay follows the reference's column model only");
     fd2_status st = fd2_wait(c);
     if (st != FD2_OK) return st;
     FD2_CUDA(c, cudaSetDevice(c->device));

@@ -672,6 +672,190 @@ struct Walker {
         return fate;
     }
 
+    // ---- explicit column lattice (options.column_grid = 1; no counterpart
+    // in the reference, whose next column is drawn at random after every
+    // crossing).  Columns are the cylinders of radius R around the square
+    // lattice points ((i + 1/2) p, (j + 1/2) p); the photon is either inside
+    // the column centred at (xc, yc) or in the gap medium between them.
+    // Walls refract and reflect with the unpolarised Fresnel coefficients on
+    // the roughened geometric normal (vector Snell law); in the gap the
+    // photon flies straight until it meets a column (traced cell by cell),
+    // the top reflector, the sensor or the detector's side.  Bulk absorption
+    // acts inside the columns only.
+    bool in_gap;
+
+    template <class G>
+    __device__ __forceinline__ void grid_place(const G &g)
+    {
+        xc = (floorf(px / g.pitch) + 0.5f) * g.pitch;
+        yc = (floorf(py / g.pitch) + 0.5f) * g.pitch;
+        const float rx = px - xc, ry = py - yc;
+        in_gap = rx * rx + ry * ry >= g.R * g.R;
+    }
+
+    // Top reflector (absorb or diffuse reflection downwards, the reference's
+    // top rule) or sensor (detect, or specular reflection with sensor_refl).
+    template <class G>
+    __device__ __forceinline__ int grid_plane(const G &g, bool top)
+    {
+        if (top) {
+            if (g.top_absfrac > 0.0f && u() < g.top_absfrac) return kAbsTop;
+            dz = -fabsf(2.0f * u() - 1.0f);
+            const float rr = sqrtf(fmaxf(0.0f, 1.0f - dz * dz));
+            float s, c;
+            __sincosf(kPi * (2.0f * u() - 1.0f), &s, &c);
+            dx = rr * c;
+            dy = rr * s;
+            return kAlive;
+        }
+        if (!(g.sensor_refl > 0.0f && u() < g.sensor_refl)) {
+            set_pixel(g);
+            return kDetect;
+        }
+        dz = -dz;
+        return kAlive;
+    }
+
+    // A wall of the column centred at (cx, cy), met at (px, py); `inside`:
+    // from within the column.  The normal toward the incident side is
+    // roughened (redrawn while the photon would not meet it); reflect with
+    // the Fresnel probability (total reflection included), else refract.
+    template <class G>
+    __device__ __forceinline__ int grid_wall(const G &g, float cx, float cy, bool inside)
+    {
+        float ox = px - cx, oy = py - cy;
+        const float inv = rsqrtf(ox * ox + oy * oy);
+        ox *= inv;
+        oy *= inv;
+        const float sgn = inside ? -1.0f : 1.0f;  // normal toward the incident medium
+        float c1 = 0.0f;
+        for (int t = 0; t < 8; ++t) {
+            top_up_inner();
+            nx = sgn * ox; ny = sgn * oy; nz = 0.0f;
+            if (g.beta > 0.0f) roughen(g.beta);
+            c1 = -(dx * nx + dy * ny + dz * nz);
+            if (c1 > 0.0f) break;
+        }
+        if (!(c1 > 0.0f)) {
+            nx = sgn * ox; ny = sgn * oy; nz = 0.0f;
+            c1 = fmaxf(-(dx * nx + dy * ny), 0.0f);
+        }
+        const float eta = inside ? g.eta_in : g.eta_out;  // n_incident / n_transmitted
+        const float st2 = eta * eta * fmaxf(0.0f, 1.0f - c1 * c1);
+        float pr = 1.0f, ct = 0.0f;
+        if (st2 < 1.0f) {
+            ct = sqrtf(1.0f - st2);
+            pr = fresnel(c1, ct, eta);
+        }
+        if (u() < pr) {
+            dx = fmaf(2.0f * c1, nx, dx);
+            dy = fmaf(2.0f * c1, ny, dy);
+            dz = fmaf(2.0f * c1, nz, dz);
+            renorm(dx, dy, dz);
+            return kAlive;
+        }
+        const float k = eta * c1 - ct;
+        dx = fmaf(eta, dx, k * nx);
+        dy = fmaf(eta, dy, k * ny);
+        dz = fmaf(eta, dz, k * nz);
+        renorm(dx, dy, dz);
+        in_gap = inside;
+        if (!inside) {
+            xc = cx;
+            yc = cy;
+        }
+        return kAlive;
+    }
+
+    // One segment of the lattice walk: a flight to the next surface and what
+    // happens there.  Draws at most 7 uniforms between ring checks.
+    template <class G>
+    __device__ __forceinline__ int grid_segment(const G &g)
+    {
+        top_up_inner();
+        if (++rebound > kMaxBoundaryCalls) return kCapped;
+        const float zp = dz > 0.0f ? g.half : -g.half;
+        const float dplane = dz != 0.0f ? (zp - pz) / dz : 3.0e38f;
+        if (!in_gap) {
+            const float ddx = px - xc, ddy = py - yc;
+            const float qa = dx * dx + dy * dy;
+            const float qb = 2.0f * (ddx * dx + ddy * dy);
+            // a photon on the wall (rounded just outside it) is on the wall:
+            // the far root then always exists
+            const float qc = fminf(ddx * ddx + ddy * ddy - g.R * g.R, 0.0f);
+            const float dw = wall_root(qa, qb, qc);
+            const bool plane = dplane <= dw;
+            const float d = fmaxf(plane ? dplane : dw, 0.0f);
+            px = fmaf(d, dx, px);
+            py = fmaf(d, dy, py);
+            pz = plane ? zp : fmaf(d, dz, pz);
+            dist += d;
+            if (g.neg_inv_mu != 0.0f) {
+                const float da = d * g.mu;
+                if (da >= budget) return kAbsBulk;
+                budget -= da;
+            }
+            if (outside_xy(g)) return kLost;
+            if (plane) return grid_plane(g, zp > 0.0f);
+            return grid_wall(g, xc, yc, true);
+        }
+        // in the gap: the first column along the ray, cell by cell (a column
+        // lies inside its own cell, so the first hit is in the first cell
+        // that holds one)
+        const float p = g.pitch;
+        float tx = 3.0e38f, ty = 3.0e38f;
+        if (dx > 0.0f) tx = (g.xdet - px) / dx;
+        else if (dx < 0.0f) tx = -px / dx;
+        if (dy > 0.0f) ty = (g.ydet - py) / dy;
+        else if (dy < 0.0f) ty = -py / dy;
+        const float tside = fminf(tx, ty);
+        const float tend = fminf(dplane, tside);
+        int i = (int)floorf(px / p), j = (int)floorf(py / p);
+        const int si = dx > 0.0f ? 1 : -1, sj = dy > 0.0f ? 1 : -1;
+        float tmx = dx != 0.0f ? (((float)(dx > 0.0f ? i + 1 : i)) * p - px) / dx : 3.0e38f;
+        float tmy = dy != 0.0f ? (((float)(dy > 0.0f ? j + 1 : j)) * p - py) / dy : 3.0e38f;
+        const float tdx = dx != 0.0f ? p / fabsf(dx) : 3.0e38f;
+        const float tdy = dy != 0.0f ? p / fabsf(dy) : 3.0e38f;
+        const float qa = dx * dx + dy * dy;
+        for (int k = 0; k < kMaxGridCells; ++k) {
+            const float cx = ((float)i + 0.5f) * p, cy = ((float)j + 0.5f) * p;
+            const float fx = px - cx, fy = py - cy;
+            const float qb = 2.0f * (fx * dx + fy * dy);
+            const float qc = fx * fx + fy * fy - g.R * g.R;
+            if (qa > 0.0f && qb < 0.0f) {
+                const float disc = qb * qb - 4.0f * qa * qc;
+                if (disc >= 0.0f) {
+                    const float t1 = (2.0f * qc) / (-qb + sqrtf(disc));  // the entry root
+                    if (t1 > 1e-4f && t1 < tend) {
+                        px = fmaf(t1, dx, px);
+                        py = fmaf(t1, dy, py);
+                        pz = fmaf(t1, dz, pz);
+                        dist += t1;
+                        return grid_wall(g, cx, cy, false);
+                    }
+                }
+            }
+            const float tn = fminf(tmx, tmy);
+            if (tn >= tend) break;
+            if (tmx < tmy) {
+                i += si;
+                tmx += tdx;
+            } else {
+                j += sj;
+                tmy += tdy;
+            }
+            if (k + 1 == kMaxGridCells) return kCapped;
+        }
+        if (dplane <= tside) {
+            px = fmaf(dplane, dx, px);
+            py = fmaf(dplane, dy, py);
+            pz = zp;
+            dist += dplane;
+            return grid_plane(g, zp > 0.0f);
+        }
+        return kLost;
+    }
+
     // One transport step (the body of the reference's step function algo):
     // flight, sensor, trapped-photon restart, or a surface interaction up to
     // the Fresnel part.  Returns the photon's fate, kAlive while it is in

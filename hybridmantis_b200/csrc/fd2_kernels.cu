@@ -339,7 +339,7 @@ struct SmemLayout {
 // the single geometry is read from the kernel parameters.  kRadial (label
 // mode): a detected photon is binned by its distance from its event into
 // the history's radial histogram instead of the PRF image.
-template <bool kMulti, int kMaxThreads, int kMinBlocks, bool kRadial = false>
+template <bool kMulti, int kMaxThreads, int kMinBlocks, bool kRadial = false, bool kGrid = false>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(const __grid_constant__ TransportArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -445,6 +445,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                     prim = __float_as_int(s.pos.w);
                     geom = (int)s.geom;
                     w.start(k, (uint32_t)(a.event_base + s.event), k == 0);
+                    if constexpr (kGrid) w.grid_place(a.g0);
                     alive = true;
                 }
                 needy &= ~__ballot_sync(kFull, mine);
@@ -461,34 +462,40 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         // Fresnel part for the parked lanes together once `fresnel_batch` of
         // them wait (or nothing else runs)
         int fate = kAlive;
-        if (alive && !parked && !xretry) {
-            fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
-            if (fate == kNeedsFresnel) {
-                parked = true;
-                fate = kAlive;
+        if constexpr (kGrid) {
+            // explicit column lattice: one segment per round per live lane
+            if (alive) fate = w.grid_segment(a.g0);
+            if (alive && fate == kAlive) w.top_up();
+        } else {
+            if (alive && !parked && !xretry) {
+                fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
+                if (fate == kNeedsFresnel) {
+                    parked = true;
+                    fate = kAlive;
+                }
             }
-        }
-        // one warp-wide refill per round, in one inlined copy, for every lane
-        // whose photon goes on: crosstalk attempts, parked lanes and the next
-        // round's step alike
-        if ((alive && fate == kAlive) || fate == kNeedsNormal) w.top_up();
-        if (alive && !parked) {
-            // crosstalk: one attempt at the next column's normal per round, so
-            // a rejected attempt is retried beside the other lanes' first ones
-            if (xretry || fate == kNeedsNormal) {
-                fate = kMulti ? w.crosstalk_normal(s_geom[geom], xtries) : w.crosstalk_normal(a.g0, xtries);
-                xretry = fate == kRetryNormal;
-                if (xretry) fate = kAlive;
-                else xtries = 0;
+            // one warp-wide refill per round, in one inlined copy, for every lane
+            // whose photon goes on: crosstalk attempts, parked lanes and the next
+            // round's step alike
+            if ((alive && fate == kAlive) || fate == kNeedsNormal) w.top_up();
+            if (alive && !parked) {
+                // crosstalk: one attempt at the next column's normal per round, so
+                // a rejected attempt is retried beside the other lanes' first ones
+                if (xretry || fate == kNeedsNormal) {
+                    fate = kMulti ? w.crosstalk_normal(s_geom[geom], xtries) : w.crosstalk_normal(a.g0, xtries);
+                    xretry = fate == kRetryNormal;
+                    if (xretry) fate = kAlive;
+                    else xtries = 0;
+                }
             }
-        }
-        const unsigned waiting = __ballot_sync(kFull, parked);
-        if (waiting) {
-            const unsigned busy = __ballot_sync(kFull, alive && !parked && fate == kAlive);
-            if ((unsigned)__popc(waiting) >= fresnel_min || busy == 0) {
-                if (parked) {
-                    fate = kMulti ? w.surface_fresnel(s_geom[geom]) : w.surface_fresnel(a.g0);
-                    parked = false;
+            const unsigned waiting = __ballot_sync(kFull, parked);
+            if (waiting) {
+                const unsigned busy = __ballot_sync(kFull, alive && !parked && fate == kAlive);
+                if ((unsigned)__popc(waiting) >= fresnel_min || busy == 0) {
+                    if (parked) {
+                        fate = kMulti ? w.surface_fresnel(s_geom[geom]) : w.surface_fresnel(a.g0);
+                        parked = false;
+                    }
                 }
             }
         }
@@ -675,12 +682,13 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
 // resident CTAs per SM (128, 85, 64 registers), blocks of 320 threads for
 // two (102 registers: 20 warps per SM; the walk fits without spills, 352
 // threads would spill), other larger blocks for one.
-#define FD2_TRANSPORT_VARIANTS(X)                          \
-    X(false, 512, 1, false) X(false, 256, 2, false)        \
-    X(false, 320, 2, false) X(true, 320, 2, false)         \
-    X(false, 256, 3, false) X(false, 256, 4, false)        \
-    X(true, 512, 1, false) X(true, 256, 2, false)          \
-    X(true, 256, 3, false) X(true, 256, 2, true)
+#define FD2_TRANSPORT_VARIANTS(X)                                        \
+    X(false, 512, 1, false, false) X(false, 256, 2, false, false)        \
+    X(false, 320, 2, false, false) X(true, 320, 2, false, false)         \
+    X(false, 256, 2, false, true) X(false, 320, 2, false, true)          \
+    X(false, 256, 3, false, false) X(false, 256, 4, false, false)        \
+    X(true, 512, 1, false, false) X(true, 256, 2, false, false)          \
+    X(true, 256, 3, false, false) X(true, 256, 2, true, false)
 
 cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
 {
@@ -694,14 +702,14 @@ cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
     if (e != cudaSuccess) return e;
     const size_t need = transport_smem_bytes(cfg, n_geom);
     // dynamic limit = opt-in maximum - the kernel's static shared memory
-#define FD2_SET_ATTR(M, T, B, R)                                                                          \
+#define FD2_SET_ATTR(M, T, B, R, L)                                                                       \
     if (e == cudaSuccess) {                                                                               \
         cudaFuncAttributes fa;                                                                            \
-        e = cudaFuncGetAttributes(&fa, transport_kernel<M, T, B, R>);                                     \
+        e = cudaFuncGetAttributes(&fa, transport_kernel<M, T, B, R, L>);                                  \
         const int lim = max_optin - (int)fa.sharedSizeBytes;                                              \
         if (e == cudaSuccess && need > (size_t)lim) e = cudaErrorInvalidValue;                            \
         if (e == cudaSuccess)                                                                             \
-            e = cudaFuncSetAttribute(transport_kernel<M, T, B, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim); \
+            e = cudaFuncSetAttribute(transport_kernel<M, T, B, R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim); \
     }
     FD2_TRANSPORT_VARIANTS(FD2_SET_ATTR)
 #undef FD2_SET_ATTR
@@ -719,7 +727,13 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
     const unsigned grid = (unsigned)(sm_count * cfg.ctas_per_sm);
     const bool multi = a.n_geom > 1;
     const int per_sm = cfg.block > 256 ? 1 : std::min(std::max(cfg.ctas_per_sm, 2), multi ? 3 : 4);
-    if (a.radial) {
+    if (a.g0.grid) {
+        // explicit column lattice: single geometry, 256 or 320 threads
+        if (multi || a.radial) return cudaErrorInvalidConfiguration;
+        if (cfg.block == 320) transport_kernel<false, 320, 2, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else if (cfg.block <= 256) transport_kernel<false, 256, 2, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else return cudaErrorInvalidConfiguration;
+    } else if (a.radial) {
         // label mode: one variant, 256 threads, two CTAs per SM
         if (cfg.block > 256) return cudaErrorInvalidConfiguration;
         transport_kernel<true, 256, 2, true><<<(unsigned)(sm_count * 2), cfg.block, smem, s>>>(a);

@@ -28,6 +28,7 @@ enum Fate : int {
 constexpr uint32_t kMaxBoundaryCalls = 1u << 20;  // boundary interactions per photon
 constexpr int kMaxSurfaceLoops = 1 << 16;         // Fresnel/hop cycles per interaction
 constexpr int kMaxTopLoops = 1 << 12;             // top/sensor ping-pong per hop
+constexpr int kMaxGridCells = 1 << 14;            // lattice cells one gap flight may cross
 
 // One detector geometry, in the float form the walk uses.
 struct DevGeom {
@@ -45,6 +46,11 @@ struct DevGeom {
     long long prf_offset;  // first PRF element of this geometry
     // the reference's float parameters, as given (used by the replay)
     float mu, n_col, n_gap, d_max;
+    // explicit column lattice (options.column_grid; no counterpart in the
+    // reference): 0 = off, 1 = square lattice of columns centred at
+    // ((i + 1/2) pitch, (j + 1/2) pitch), pitch = 2 R + gap
+    int grid;
+    float pitch;
 };
 
 }  // namespace fd2

@@ -23,11 +23,14 @@ def main():
     ap.add_argument("--refill", type=int, default=0)
     ap.add_argument("--window", type=int, default=-1)
     ap.add_argument("--fresnel", type=int, default=0)
+    ap.add_argument("--grid", type=int, default=0, help="1: explicit square column lattice")
+    ap.add_argument("--gap", type=float, default=0.5, help="lattice gap between columns (um)")
     a = ap.parse_args()
     es = fd.synth_events(a.config, a.xrays, a.seed)
     x, y, z = es.to_cm()
     with fd.OpticalTransport(es.params, block_size=a.block, ctas_per_sm=a.ctas, chunk=a.chunk, refill=a.refill,
-                             prf_window=a.window, fresnel_batch=a.fresnel) as t:
+                             prf_window=a.window, fresnel_batch=a.fresnel, column_grid=a.grid,
+                             grid_gap_um=a.gap) as t:
         t.submit_events(x, y, z, es.e_ev.astype(np.float64), es.hist)
         out = []
         for _ in range(a.runs):
@@ -35,7 +38,12 @@ def main():
             tm = t.timing()
             out.append({"transport_ms": tm["transport_ms"], "photons": tm["photons"],
                         "photons_per_s": tm["photons"] / (tm["transport_ms"] * 1e-3)})
-        print(json.dumps({"events": es.n, "runs": out, "launch": {k: tm[k] for k in
+        c = t.counters()
+        st = t.phs_stats()
+        n = max(c["generated"], 1)
+        fates = {k: c[k] / n for k in ("detected", "abs_top", "abs_bulk", "lost", "capped")}
+        print(json.dumps({"events": es.n, "runs": out, "fates": fates, "phs_mean": st["mean"], "swank": st["swank"],
+                          "launch": {k: tm[k] for k in
                                                                  ("grid", "block", "chunk", "refill", "prf_window",
                                                                                   "fresnel_batch")}}))
 

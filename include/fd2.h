@@ -132,6 +132,16 @@ typedef struct fd2_options {
                                       r_max ((j+1)/bins)^2, bin radial_bins is
                                       r >= r_max = radial_max_um (fd2_get_radial) */
     double radial_max_um;
+    int32_t column_grid;           /* 0: the reference's column model (after each
+                                      crossing the next column's orientation is
+                                      drawn at random, hops U(d_min, d_max));
+                                      1: an explicit square lattice of columns
+                                      of pitch 2 radius + grid_gap_um, with
+                                      Fresnel refraction at every wall and
+                                      straight flights through the gap (no
+                                      counterpart in the reference; single
+                                      geometry, production transport only)  */
+    double grid_gap_um;            /* lattice: gap between neighbouring columns */
 } fd2_options;
 
 typedef struct fd2_counters {
