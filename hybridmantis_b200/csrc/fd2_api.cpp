@@ -556,7 +556,7 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     if (c->opt.max_photons_per_event <= 0) c->opt.max_photons_per_event = 900000;
     if (c->opt.event_base < 0 || c->opt.radial_bins < 0 || c->opt.radial_bins > 4096 ||
         (c->opt.radial_bins > 0 && !(c->opt.radial_max_um > 0.0)) || c->opt.column_grid < 0 ||
-        c->opt.column_grid > 1 || (c->opt.column_grid && (!(c->opt.grid_gap_um > 0.0) || c->opt.radial_bins > 0))) {
+        c->opt.column_grid > 2 || (c->opt.column_grid && (!(c->opt.grid_gap_um > 0.0) || c->opt.radial_bins > 0))) {
         delete c;
         return FD2_ERR_INVALID_ARGUMENT;
     }

@@ -672,11 +672,13 @@ struct Walker {
         return fate;
     }
 
-    // ---- explicit column lattice (options.column_grid = 1; no counterpart
-    // in the reference, whose next column is drawn at random after every
-    // crossing).  Columns are the cylinders of radius R around the square
-    // lattice points ((i + 1/2) p, (j + 1/2) p); the photon is either inside
-    // the column centred at (xc, yc) or in the gap medium between them.
+    // ---- explicit column lattice (options.column_grid = 1 or 2; no
+    // counterpart in the reference, whose next column is drawn at random
+    // after every crossing).  Columns are the cylinders of radius R around
+    // the square lattice points ((i + 1/2) p, (j + 1/2) p), or around the
+    // hexagonal lattice points ((i + 1/2) p + o_j, (j + 1/2) h), h = p sqrt(3)/2,
+    // o_j = p/2 on odd rows; the photon is either inside the column centred at
+    // (xc, yc) or in the gap medium between them.
     // Walls refract and reflect with the unpolarised Fresnel coefficients on
     // the roughened geometric normal (vector Snell law); in the gap the
     // photon flies straight until it meets a column (traced cell by cell),
@@ -687,10 +689,49 @@ struct Walker {
     template <class G>
     __device__ __forceinline__ void grid_place(const G &g)
     {
+        if (g.grid == 2) {
+            // the nearest of the brick's own column and its four diagonal
+            // neighbours in the rows above and below
+            const float h = g.pitch * 0.8660254037844386f;
+            const int j = (int)floorf(py / h);
+            const float o = (j & 1) ? 0.5f * g.pitch : 0.0f;
+            const int i = (int)floorf((px - o) / g.pitch);
+            float bx = 0.0f, by = 0.0f, bd = 3.0e38f;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                float cx, cy;
+                hex_candidate(g, i, j, q, cx, cy);
+                const float d2 = (px - cx) * (px - cx) + (py - cy) * (py - cy);
+                if (d2 < bd) { bd = d2; bx = cx; by = cy; }
+            }
+            xc = bx;
+            yc = by;
+            in_gap = bd >= g.R * g.R;
+            return;
+        }
         xc = (floorf(px / g.pitch) + 0.5f) * g.pitch;
         yc = (floorf(py / g.pitch) + 0.5f) * g.pitch;
         const float rx = px - xc, ry = py - yc;
         in_gap = rx * rx + ry * ry >= g.R * g.R;
+    }
+
+    // Hexagonal lattice: the rows are strips of height h; in row j the
+    // bricks [i p + o_j, (i + 1) p + o_j) each hold one column at their
+    // centre.  A column reaches at most R < p/2 sideways but may reach past
+    // its strip (R > h/2 when the gap is small), so the columns that
+    // overlap brick (i, j) are its own (q = 0) and the four centred on its
+    // corners' columns in rows j - 1 and j + 1 (q = 1..4).
+    template <class G>
+    __device__ __forceinline__ static void hex_candidate(const G &g, int i, int j, int q, float &cx, float &cy)
+    {
+        const float p = g.pitch, h = p * 0.8660254037844386f;
+        const float o = (j & 1) ? 0.5f * p : 0.0f;
+        cx = ((float)i + 0.5f) * p + o;
+        cy = ((float)j + 0.5f) * h;
+        if (q > 0) {
+            cy += q <= 2 ? h : -h;
+            cx += (q & 1) ? -0.5f * p : 0.5f * p;
+        }
     }
 
     // Top reflector (absorb or diffuse reflection downwards, the reference's
@@ -810,6 +851,67 @@ struct Walker {
         else if (dy < 0.0f) ty = -py / dy;
         const float tside = fminf(tx, ty);
         const float tend = fminf(dplane, tside);
+        if (g.grid == 2) {
+            // brick by brick; a hit counts in the brick where it lies
+            const float h = p * 0.8660254037844386f;
+            int j = (int)floorf(py / h);
+            int i = (int)floorf((px - ((j & 1) ? 0.5f * p : 0.0f)) / p);
+            const float qa = dx * dx + dy * dy;
+            float tin = 0.0f;
+            for (int k = 0; k < kMaxGridCells; ++k) {
+                const float o = (j & 1) ? 0.5f * p : 0.0f;
+                const float xl = (float)i * p + o;
+                const float tX = dx > 0.0f ? (xl + p - px) / dx : dx < 0.0f ? (xl - px) / dx : 3.0e38f;
+                const float tY = dy > 0.0f ? ((float)(j + 1) * h - py) / dy : dy < 0.0f ? ((float)j * h - py) / dy : 3.0e38f;
+                const float tout = fminf(tX, tY);
+                float tb = 3.0e38f, bx = 0.0f, by = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    float cx, cy;
+                    hex_candidate(g, i, j, q, cx, cy);
+                    const float fx = px - cx, fy = py - cy;
+                    const float qb = 2.0f * (fx * dx + fy * dy);
+                    const float qc = fx * fx + fy * fy - g.R * g.R;
+                    if (qa > 0.0f && qb < 0.0f) {
+                        const float disc = qb * qb - 4.0f * qa * qc;
+                        if (disc >= 0.0f) {
+                            const float t1 = (2.0f * qc) / (-qb + sqrtf(disc));
+                            if (t1 > 1e-4f && t1 >= tin - 1e-4f && t1 <= tout + 1e-4f && t1 < tb) {
+                                tb = t1;
+                                bx = cx;
+                                by = cy;
+                            }
+                        }
+                    }
+                }
+                if (tb < tend) {
+                    px = fmaf(tb, dx, px);
+                    py = fmaf(tb, dy, py);
+                    pz = fmaf(tb, dz, pz);
+                    dist += tb;
+                    return grid_wall(g, bx, by, false);
+                }
+                if (tout >= tend) break;
+                if (tX < tY) {
+                    i += dx > 0.0f ? 1 : -1;
+                } else {
+                    // the next row: the brick under the crossing point
+                    j += dy > 0.0f ? 1 : -1;
+                    const float xo = fmaf(tout, dx, px) - ((j & 1) ? 0.5f * p : 0.0f);
+                    i = (int)floorf(xo / p);
+                }
+                tin = tout;
+                if (k + 1 == kMaxGridCells) return kCapped;
+            }
+            if (dplane <= tside) {
+                px = fmaf(dplane, dx, px);
+                py = fmaf(dplane, dy, py);
+                pz = zp;
+                dist += dplane;
+                return grid_plane(g, zp > 0.0f);
+            }
+            return kLost;
+        }
         int i = (int)floorf(px / p), j = (int)floorf(py / p);
         const int si = dx > 0.0f ? 1 : -1, sj = dy > 0.0f ? 1 : -1;
         float tmx = dx != 0.0f ? (((float)(dx > 0.0f ? i + 1 : i)) * p - px) / dx : 3.0e38f;

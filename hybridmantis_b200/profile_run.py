@@ -23,7 +23,7 @@ def main():
     ap.add_argument("--refill", type=int, default=0)
     ap.add_argument("--window", type=int, default=-1)
     ap.add_argument("--fresnel", type=int, default=0)
-    ap.add_argument("--grid", type=int, default=0, help="1: explicit square column lattice")
+    ap.add_argument("--grid", type=int, default=0, help="1 / 2: explicit square / hexagonal column lattice")
     ap.add_argument("--gap", type=float, default=0.5, help="lattice gap between columns (um)")
     a = ap.parse_args()
     es = fd.synth_events(a.config, a.xrays, a.seed)

@@ -135,8 +135,10 @@ typedef struct fd2_options {
     int32_t column_grid;           /* 0: the reference's column model (after each
                                       crossing the next column's orientation is
                                       drawn at random, hops U(d_min, d_max));
-                                      1: an explicit square lattice of columns
-                                      of pitch 2 radius + grid_gap_um, with
+                                      1 / 2: an explicit square / hexagonal
+                                      lattice of columns of pitch (nearest-
+                                      neighbour distance) 2 radius +
+                                      grid_gap_um, with
                                       Fresnel refraction at every wall and
                                       straight flights through the gap (no
                                       counterpart in the reference; single

@@ -14,7 +14,9 @@
  * RoughSurface), the top reflector's diffuse downward reflection and the
  * sensor rule (boundary_analysis / detection), and the PRF pixel rule.
  *
- * Lattice: columns of radius R around ((i + 1/2) p, (j + 1/2) p), pitch p.
+ * Lattice: columns of radius R around ((i + 1/2) p, (j + 1/2) p), pitch p
+ * (square), or around ((i + 1/2) p + o_j, (j + 1/2) h), h = p sqrt(3)/2,
+ * o_j = p/2 on odd rows (hexagonal).
  * Inside a column: flight to the wall or to the top / sensor plane, bulk
  * absorption against an Exp(1) budget of absorption lengths.  At a wall:
  * the normal toward the incident medium, roughened (up to 8 draws until the
@@ -31,6 +33,7 @@ typedef struct {
     double xdet, ydet, H, R, pitch, n_col, n_gap, top_absfrac, mu, beta, sensor_refl;
     double lb_x, lb_y, ub_x, ub_y;
     int32_t pixel, xdim, ydim;
+    int32_t lattice; /* 1 square, 2 hexagonal */
 } go_geom;
 
 enum { DETECT = 0, ABS_TOP = 1, ABS_BULK = 2, LOST = 3, CAPPED = 6, ALIVE = -1 };
@@ -183,11 +186,78 @@ static int wall(photon_t *ph, const go_geom *g, double cx, double cy, int inside
     return ALIVE;
 }
 
+/* Hexagonal lattice: brick (i, j) of row j holds the column at its centre;
+ * q = 0 is that column, q = 1..4 the columns of rows j +- 1 centred on its
+ * corners' x (the only other columns that reach into the brick). */
+static void hex_candidate(const go_geom *g, int i, int j, int q, double *cx, double *cy)
+{
+    const double p = g->pitch, h = p * sqrt(3.0) / 2.0;
+    const double o = (j & 1) ? 0.5 * p : 0.0;
+    *cx = (i + 0.5) * p + o;
+    *cy = (j + 0.5) * h;
+    if (q > 0) {
+        *cy += q <= 2 ? h : -h;
+        *cx += (q & 1) ? -0.5 * p : 0.5 * p;
+    }
+}
+
+static int hex_first_hit(const go_geom *g, double px, double py, double dx, double dy, double tend, double *t_out,
+                         double *cx_out, double *cy_out)
+{
+    const double p = g->pitch, h = p * sqrt(3.0) / 2.0;
+    int j = (int)floor(py / h);
+    int i = (int)floor((px - ((j & 1) ? 0.5 * p : 0.0)) / p);
+    const double qa = dx * dx + dy * dy;
+    double tin = 0.0;
+    for (int k = 0; k < (1 << 14); ++k) {
+        const double o = (j & 1) ? 0.5 * p : 0.0;
+        const double xl = i * p + o;
+        const double tX = dx > 0.0 ? (xl + p - px) / dx : dx < 0.0 ? (xl - px) / dx : INFINITY;
+        const double tY = dy > 0.0 ? ((j + 1) * h - py) / dy : dy < 0.0 ? (j * h - py) / dy : INFINITY;
+        const double tout = fmin(tX, tY);
+        double tb = INFINITY, bx = 0.0, by = 0.0;
+        for (int q = 0; q < 5; ++q) {
+            double cx, cy;
+            hex_candidate(g, i, j, q, &cx, &cy);
+            const double fx = px - cx, fy = py - cy;
+            const double qb = 2.0 * (fx * dx + fy * dy);
+            const double qc = fx * fx + fy * fy - g->R * g->R;
+            if (qa > 0.0 && qb < 0.0) {
+                const double disc = qb * qb - 4.0 * qa * qc;
+                if (disc >= 0.0) {
+                    const double t1 = (2.0 * qc) / (-qb + sqrt(disc));
+                    if (t1 > 1e-4 && t1 >= tin - 1e-4 && t1 <= tout + 1e-4 && t1 < tb) {
+                        tb = t1;
+                        bx = cx;
+                        by = cy;
+                    }
+                }
+            }
+        }
+        if (tb < tend) {
+            *t_out = tb;
+            *cx_out = bx;
+            *cy_out = by;
+            return 1;
+        }
+        if (tout >= tend) return 0;
+        if (tX < tY) {
+            i += dx > 0.0 ? 1 : -1;
+        } else {
+            j += dy > 0.0 ? 1 : -1;
+            i = (int)floor((px + tout * dx - ((j & 1) ? 0.5 * p : 0.0)) / p);
+        }
+        tin = tout;
+    }
+    return -1;
+}
+
 /* The first column met by a gap flight from (px, py) along (dx, dy) before
  * path length tend; 1 and (t, cx, cy) when there is one. */
 int go_first_hit(const go_geom *g, double px, double py, double dx, double dy, double tend, double *t_out,
                  double *cx_out, double *cy_out)
 {
+    if (g->lattice == 2) return hex_first_hit(g, px, py, dx, dy, tend, t_out, cx_out, cy_out);
     const double p = g->pitch;
     int i = (int)floor(px / p), j = (int)floor(py / p);
     const int si = dx > 0.0 ? 1 : -1, sj = dy > 0.0 ? 1 : -1;
@@ -309,10 +379,28 @@ int go_run(const go_geom *g, int64_t n, const double *x, const double *y, const 
             ph.dz = c;
             renorm(&ph.dx, &ph.dy, &ph.dz);
             ph.budget = -log(unif(&ph.rng));
-            ph.xc = (floor(ph.px / g->pitch) + 0.5) * g->pitch;
-            ph.yc = (floor(ph.py / g->pitch) + 0.5) * g->pitch;
-            const double rx = ph.px - ph.xc, ry = ph.py - ph.yc;
-            ph.in_gap = rx * rx + ry * ry >= g->R * g->R;
+            if (g->lattice == 2) {
+                const double h = g->pitch * sqrt(3.0) / 2.0;
+                const int j = (int)floor(ph.py / h);
+                const int i = (int)floor((ph.px - ((j & 1) ? 0.5 * g->pitch : 0.0)) / g->pitch);
+                double bd = INFINITY;
+                for (int q = 0; q < 5; ++q) {
+                    double cx, cy;
+                    hex_candidate(g, i, j, q, &cx, &cy);
+                    const double d2 = (ph.px - cx) * (ph.px - cx) + (ph.py - cy) * (ph.py - cy);
+                    if (d2 < bd) {
+                        bd = d2;
+                        ph.xc = cx;
+                        ph.yc = cy;
+                    }
+                }
+                ph.in_gap = bd >= g->R * g->R;
+            } else {
+                ph.xc = (floor(ph.px / g->pitch) + 0.5) * g->pitch;
+                ph.yc = (floor(ph.py / g->pitch) + 0.5) * g->pitch;
+                const double rx = ph.px - ph.xc, ry = ph.py - ph.yc;
+                ph.in_gap = rx * rx + ry * ry >= g->R * g->R;
+            }
             int fate = ALIVE;
             while (fate == ALIVE) fate = segment(&ph, g);
             counters[0] += 1;

@@ -19,7 +19,8 @@ _lib = None
 class GoGeom(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("xdet", "ydet", "H", "R", "pitch", "n_col", "n_gap", "top_absfrac",
                                                "mu", "beta", "sensor_refl", "lb_x", "lb_y", "ub_x", "ub_y")] + \
-               [("pixel", ctypes.c_int32), ("xdim", ctypes.c_int32), ("ydim", ctypes.c_int32)]
+               [("pixel", ctypes.c_int32), ("xdim", ctypes.c_int32), ("ydim", ctypes.c_int32),
+                ("lattice", ctypes.c_int32)]
 
 
 def load():
@@ -36,12 +37,13 @@ def load():
     return _lib
 
 
-def geometry(p, gap_um: float, xdim: int, ydim: int) -> GoGeom:
-    """The lattice geometry of fd2 params `p` (hybridmantis_b200 Params)."""
+def geometry(p, gap_um: float, xdim: int, ydim: int, lattice: int = 1) -> GoGeom:
+    """The lattice geometry of fd2 params `p` (hybridmantis_b200 Params);
+    lattice 1 square, 2 hexagonal."""
     return GoGeom(xdet=p.det_x, ydet=p.det_y, H=p.det_height, R=p.radius, pitch=2 * p.radius + gap_um,
                   n_col=p.n_col, n_gap=p.n_gap, top_absfrac=p.top_absfrac, mu=p.bulk_abs, beta=p.beta,
                   sensor_refl=p.sensor_refl, lb_x=p.lb_x, lb_y=p.lb_y, ub_x=p.ub_x, ub_y=p.ub_y, pixel=p.pixel,
-                  xdim=xdim, ydim=ydim)
+                  xdim=xdim, ydim=ydim, lattice=lattice)
 
 
 def first_hit(g: GoGeom, px, py, dx, dy, tend):

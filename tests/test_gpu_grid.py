@@ -1,4 +1,5 @@
-"""The explicit column lattice (fd2_options.column_grid = 1) on the GPU.
+"""The explicit column lattices (fd2_options.column_grid = 1 square, 2
+hexagonal) on the GPU.
 
 The lattice has no counterpart in the reference (whose next column is drawn
 at random after each crossing), so it is checked against its own CPU oracle
@@ -28,23 +29,25 @@ pytestmark = pytest.mark.gpu
 FATES = ["detected", "abs_top", "abs_bulk", "lost", "capped"]
 
 
-def run_grid(es, N, gap=0.5, **kw):
-    t = hb.OpticalTransport(es.params, count_mode=hb.COUNT_GIVEN, column_grid=1, grid_gap_um=gap, **kw)
+def run_grid(es, N, gap=0.5, kind=1, **kw):
+    t = hb.OpticalTransport(es.params, count_mode=hb.COUNT_GIVEN, column_grid=kind, grid_gap_um=gap, **kw)
     t.submit(es, nphot=N)
     t.run_sync()
     return t
 
 
-def test_lattice_matches_its_oracle(require_gpu):
+@pytest.mark.parametrize("kind", [1, 2])
+def test_lattice_matches_its_oracle(require_gpu, kind):
     es, N = c0_events(80, seed=12)
     p = es.params
     n = int(N.sum())
-    with run_grid(es, N, seed=21) as t:
+    with run_grid(es, N, seed=21, kind=kind) as t:
         c = t.counters()
         prim = t.detected_per_primary()
         img = t.prf()
     xd, yd = img.shape
-    oc, oimg, oprim = go.run(go.geometry(p, 0.5, xd, yd), es.x_um, es.y_um, es.z_um, es.hist, N, p.num_hist, seed=5)
+    oc, oimg, oprim = go.run(go.geometry(p, 0.5, xd, yd, kind), es.x_um, es.y_um, es.z_um, es.hist, N, p.num_hist,
+                             seed=5)
     assert c["generated"] == oc["generated"] == n
     zs = {k: float(z_binomial(c[k], n, oc[k], n)) for k in FATES}
     g, o = phs_moments(prim), phs_moments(oprim)
@@ -54,14 +57,15 @@ def test_lattice_matches_its_oracle(require_gpu):
     chi2, dof = poisson_chi2(radial_profile(img, 250.5, 250.5, edges), radial_profile(oimg, 250.5, 250.5, edges))
     rep = {"z_fates": zs, "gpu": {k: c[k] / n for k in FATES}, "oracle": {k: oc[k] / n for k in FATES},
            "z_mean": z_mean, "z_swank": z_swank, "radial_chi2": chi2, "dof": dof}
-    report("grid_vs_oracle_c0", rep)
+    report(f"grid_vs_oracle_c0_lattice{kind}", rep)
     for k, z in zs.items():
         assert abs(z) < 5.0, rep
     assert abs(z_mean) < 5.0 and abs(z_swank) < 5.0, rep
     assert chi2 < dof + 6 * np.sqrt(2 * dof), rep
 
 
-def test_index_matched_lattice_is_invisible(require_gpu):
+@pytest.mark.parametrize("kind", [1, 2])
+def test_index_matched_lattice_is_invisible(require_gpu, kind):
     p = hb.default_params()
     p.radius, p.n_col, p.n_gap, p.top_absfrac, p.bulk_abs, p.beta = 5.0, 1.8, 1.8, 1.0, 0.0, 0.3
     es = hb.synth_events(0, 1, 1)
@@ -71,7 +75,7 @@ def test_index_matched_lattice_is_invisible(require_gpu):
     es.y_um[:] = y0
     es.z_um[:] = z0
     n = 600_000
-    with run_grid(es, np.array([n], np.int32)) as t:
+    with run_grid(es, np.array([n], np.int32), kind=kind) as t:
         c = t.counters()
     expect = straight_line_detected_fraction(x0, y0, z0 + p.det_height / 2, p.det_x)
     got = c["detected"] / n
@@ -79,11 +83,12 @@ def test_index_matched_lattice_is_invisible(require_gpu):
     assert c["abs_bulk"] == 0 and c["capped"] == 0
 
 
-def test_lattice_results_independent_of_launch_shape(require_gpu):
+@pytest.mark.parametrize("kind", [1, 2])
+def test_lattice_results_independent_of_launch_shape(require_gpu, kind):
     es, N = c0_events(32, seed=3)
     outs = []
     for kw in (dict(), dict(block_size=256, chunk=8, refill=8, prf_window=0), dict(block_size=128, use_graph=False)):
-        with run_grid(es, N, seed=4, **kw) as t:
+        with run_grid(es, N, seed=4, kind=kind, **kw) as t:
             c = t.counters()
             c.pop("photon_distance")
             outs.append((c, t.detected_per_primary().copy(), t.prf().copy()))
