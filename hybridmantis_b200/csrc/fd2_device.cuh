@@ -808,13 +808,12 @@ struct Walker {
         return kAlive;
     }
 
-    // One segment of the lattice walk: a flight to the next surface and what
-    // happens there.  Draws at most 7 uniforms between ring checks.
+    // The flight of a lattice segment: to a plane (kToPlane), to the wall of
+    // the column at (wx, wy) (kToWall; win: from inside it), or a fate.
+    static constexpr int kToPlane = 200, kToWall = 201;
     template <class G>
-    __device__ __forceinline__ int grid_segment(const G &g)
+    __device__ __forceinline__ int grid_flight(const G &g, float &wx, float &wy, bool &win)
     {
-        top_up_inner();
-        if (++rebound > kMaxBoundaryCalls) return kCapped;
         const float zp = dz > 0.0f ? g.half : -g.half;
         const float dplane = dz != 0.0f ? (zp - pz) / dz : 3.0e38f;
         if (!in_gap) {
@@ -837,8 +836,11 @@ struct Walker {
                 budget -= da;
             }
             if (outside_xy(g)) return kLost;
-            if (plane) return grid_plane(g, zp > 0.0f);
-            return grid_wall(g, xc, yc, true);
+            if (plane) return kToPlane;
+            wx = xc;
+            wy = yc;
+            win = true;
+            return kToWall;
         }
         // in the gap: the first column along the ray, cell by cell (a column
         // lies inside its own cell, so the first hit is in the first cell
@@ -889,7 +891,10 @@ struct Walker {
                     py = fmaf(tb, dy, py);
                     pz = fmaf(tb, dz, pz);
                     dist += tb;
-                    return grid_wall(g, bx, by, false);
+                    wx = bx;
+                    wy = by;
+                    win = false;
+                    return kToWall;
                 }
                 if (tout >= tend) break;
                 if (tX < tY) {
@@ -908,7 +913,7 @@ struct Walker {
                 py = fmaf(dplane, dy, py);
                 pz = zp;
                 dist += dplane;
-                return grid_plane(g, zp > 0.0f);
+                return kToPlane;
             }
             return kLost;
         }
@@ -933,7 +938,10 @@ struct Walker {
                         py = fmaf(t1, dy, py);
                         pz = fmaf(t1, dz, pz);
                         dist += t1;
-                        return grid_wall(g, cx, cy, false);
+                        wx = cx;
+                        wy = cy;
+                        win = false;
+                        return kToWall;
                     }
                 }
             }
@@ -953,9 +961,25 @@ struct Walker {
             py = fmaf(dplane, dy, py);
             pz = zp;
             dist += dplane;
-            return grid_plane(g, zp > 0.0f);
+            return kToPlane;
         }
         return kLost;
+    }
+
+    // One segment of the lattice walk: a flight to the next surface and what
+    // happens there, the interaction in one place for lanes in either medium.
+    // Draws at most 7 uniforms between ring checks.
+    template <class G>
+    __device__ __forceinline__ int grid_segment(const G &g)
+    {
+        top_up_inner();
+        if (++rebound > kMaxBoundaryCalls) return kCapped;
+        float wx = 0.0f, wy = 0.0f;
+        bool win = false;
+        const int f = grid_flight(g, wx, wy, win);
+        if (f == kToPlane) return grid_plane(g, pz > 0.0f);
+        if (f == kToWall) return grid_wall(g, wx, wy, win);
+        return f;
     }
 
     // One transport step (the body of the reference's step function algo):
