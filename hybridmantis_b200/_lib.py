@@ -131,6 +131,41 @@ class SgStats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class XrayMaterialInfo(ctypes.Structure):
+    _fields_ = [("density_g_cm3", ctypes.c_double), ("molar_mass_g_mol", ctypes.c_double),
+                ("molecules_per_cm3", ctypes.c_double), ("n_elements", ctypes.c_int32),
+                ("z", ctypes.c_int32 * 8), ("atoms_per_molecule", ctypes.c_double * 8),
+                ("k_edge_ev", ctypes.c_double * 8), ("e_min_ev", ctypes.c_double), ("e_max_ev", ctypes.c_double),
+                ("n_photon_nodes", ctypes.c_int32), ("n_transitions", ctypes.c_int32),
+                ("rayleigh_screening_cm", ctypes.c_double)]
+
+
+class XraySource(ctypes.Structure):
+    _fields_ = [("particle", ctypes.c_int32), ("n_spectrum", ctypes.c_int32), ("e_ev", ctypes.c_void_p),
+                ("prob", ctypes.c_void_p), ("center_cm", ctypes.c_double * 3), ("sides_cm", ctypes.c_double * 3),
+                ("euler_deg", ctypes.c_double * 3), ("direction", ctypes.c_double * 3),
+                ("semiaperture_deg", ctypes.c_double)]
+
+
+class XrayOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("det_x_um", ctypes.c_double), ("det_y_um", ctypes.c_double),
+                ("det_height_um", ctypes.c_double), ("eabs_electron_ev", ctypes.c_double),
+                ("eabs_photon_ev", ctypes.c_double), ("electron_step_loss", ctypes.c_double),
+                ("electron_local_ev", ctypes.c_double), ("fluorescence", ctypes.c_int32), ("max_edes_per_history", ctypes.c_int32),
+                ("batch_histories", ctypes.c_int64), ("seed", ctypes.c_uint64)]
+
+
+class XrayStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ["histories", "missed", "edes", "merged_histories", "photoelectric",
+                                              "compton", "rayleigh", "fluorescence_emitted",
+                                              "fluorescence_escaped", "auger_emitted", "electron_steps"]] + \
+               [(n, ctypes.c_double) for n in ["e_source_ev", "e_deposited_ev", "e_escaped_photon_ev",
+                                               "e_escaped_electron_ev"]]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _lib = None
 
 # Every symbol include/*.h declare.
@@ -151,6 +186,12 @@ EXPORTED = [
     "fd2_sg_get_hull", "fd2_sg_set_hull", "fd2_sg_save", "fd2_sg_load", "fd2_sg_loss_grad", "fd2_sg_predict",
     "fd2_sg_run",
     "fd2_mtf", "fd2_nnps",
+    "fd2_submit_events_device",
+    "fd2_xray_load_material", "fd2_xray_save_material", "fd2_xray_free_material", "fd2_xray_material_get_info",
+    "fd2_xray_attenuation", "fd2_xray_electron_tables", "fd2_xray_default_options", "fd2_xray_create",
+    "fd2_xray_destroy", "fd2_xray_last_error", "fd2_xray_run", "fd2_xray_num_edes", "fd2_xray_get_edes",
+    "fd2_xray_get_history_info", "fd2_xray_get_stats", "fd2_xray_clear_stats", "fd2_xray_get_timing",
+    "fd2_xray_submit", "fd2_xray_device_edes", "fd2_xray_sample",
 ]
 
 
@@ -233,6 +274,28 @@ def load():
         "fd2_nnps": (ctypes.c_int, [ctypes.c_int32, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                     ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                     ctypes.c_int32, vp, vp, vp, P(ctypes.c_double)]),
+        "fd2_submit_events_device": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int64]),
+        "fd2_xray_load_material": (ctypes.c_int, [ctypes.c_char_p, P(vp)]),
+        "fd2_xray_save_material": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "fd2_xray_free_material": (None, [vp]),
+        "fd2_xray_material_get_info": (ctypes.c_int, [vp, P(XrayMaterialInfo)]),
+        "fd2_xray_attenuation": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp]),
+        "fd2_xray_electron_tables": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp, vp]),
+        "fd2_xray_default_options": (None, [P(XrayOptions)]),
+        "fd2_xray_create": (ctypes.c_int, [vp, P(XrayOptions), P(vp)]),
+        "fd2_xray_destroy": (None, [vp]),
+        "fd2_xray_last_error": (ctypes.c_char_p, [vp]),
+        "fd2_xray_run": (ctypes.c_int, [vp, P(XraySource), ctypes.c_int64, ctypes.c_int64]),
+        "fd2_xray_num_edes": (ctypes.c_int, [vp, P(ctypes.c_int64)]),
+        "fd2_xray_get_edes": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int64]),
+        "fd2_xray_get_history_info": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_int64]),
+        "fd2_xray_get_stats": (ctypes.c_int, [vp, P(XrayStats)]),
+        "fd2_xray_clear_stats": (ctypes.c_int, [vp]),
+        "fd2_xray_get_timing": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_double)]),
+        "fd2_xray_submit": (ctypes.c_int, [vp, vp]),
+        "fd2_xray_device_edes": (ctypes.c_int, [vp, P(vp), P(vp), P(vp), P(vp), P(vp), P(ctypes.c_int64)]),
+        "fd2_xray_sample": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                           ctypes.c_uint64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

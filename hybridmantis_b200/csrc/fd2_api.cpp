@@ -211,7 +211,9 @@ fd2_status check_status(fd2_ctx *c)
 
 void fit_window(fd2_ctx *c);
 
-void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *geom, int64_t n)
+// The PRF window around the mean position (um) of geometry 0's k events,
+// given as coordinate sums.
+void choose_window_sums(fd2_ctx *c, double sx, double sy, int64_t k)
 {
     const DevGeom &g = c->dgeoms[0];
     int w = c->opt.prf_window;
@@ -220,6 +222,15 @@ void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *g
     if (w > g.xdim) w = g.xdim;
     if (w > g.ydim) w = g.ydim;
     if (w > 176) w = 176;  // fits beside the rings in shared memory
+    c->cfg.window = c->win_chosen = (k > 0 && w >= 16) ? w : 0;
+    if (!c->cfg.window) return;
+    c->win_cx = (int)std::floor((sx / (double)k - g.lb_x) / g.pixel);
+    c->win_cy = (int)std::floor((sy / (double)k - g.lb_y) / g.pixel);
+    fit_window(c);
+}
+
+void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *geom, int64_t n)
+{
     double sx = 0, sy = 0;
     int64_t k = 0;
     for (int64_t i = 0; i < n; ++i) {
@@ -228,11 +239,7 @@ void choose_window(fd2_ctx *c, const float *x, const float *y, const uint16_t *g
         sy += y[i];
         ++k;
     }
-    c->cfg.window = c->win_chosen = (k > 0 && w >= 16) ? w : 0;
-    if (!c->cfg.window) return;
-    c->win_cx = (int)std::floor((sx / (double)k - g.lb_x) / g.pixel);
-    c->win_cy = (int)std::floor((sy / (double)k - g.lb_y) / g.pixel);
-    fit_window(c);
+    choose_window_sums(c, sx, sy, k);
 }
 
 fd2::TransportArgs transport_args(fd2_ctx *c)
@@ -669,7 +676,11 @@ fd2_status fd2_set_geometries(fd2_ctx *c, const fd2_geometry *g, int32_t n)
     return set_config(c, c->cfg);
 }
 
-static fd2_status submit_common(fd2_ctx *c, int64_t n, const float *xs, const float *ys, const uint16_t *geom)
+// What every submission does once the events are on the device: the PRF
+// window (from positions xs, ys, or from the coordinate sums when xs is
+// null), the work-queue capacity and, for given counts, the count pass.
+static fd2_status submit_common(fd2_ctx *c, int64_t n, const float *xs, const float *ys, const uint16_t *geom,
+                                const double *sums = nullptr)
 {
     c->n_events = n;
     c->counts_ready = false;
@@ -679,7 +690,8 @@ static fd2_status submit_common(fd2_ctx *c, int64_t n, const float *xs, const fl
     const size_t G = c->geoms.size();
     c->hist_per_geom.assign(G, 0.0);
     if (G == 1) c->hist_per_geom[0] = c->params.num_hist;
-    choose_window(c, xs, ys, geom, n);
+    if (xs) choose_window(c, xs, ys, geom, n);
+    else choose_window_sums(c, sums ? sums[0] : 0.0, sums ? sums[1] : 0.0, n);
     fd2_status st = ensure_chunks(c);
     if (st != FD2_OK) return st;
     FD2_CUDA(c, fd2::prepare_transport(c->cfg, (int)G));
@@ -741,6 +753,49 @@ fd2_status fd2_submit_events(fd2_ctx *c, const double *x_cm, const double *y_cm,
     }
     c->mu_total = mu;
     return submit_common(c, n, xs.data(), ys.data(), nullptr);
+}
+
+fd2_status fd2_submit_events_device(fd2_ctx *c, const double *x_cm, const double *y_cm, const double *z_cm,
+                                    const double *de_ev, const int32_t *hist, int64_t n)
+{
+    if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
+    if (!c || n < 0 || (n > 0 && (!x_cm || !y_cm || !z_cm || !de_ev || !hist)) || n >= ((int64_t)1 << 31))
+        return fail(c, FD2_ERR_INVALID_ARGUMENT, "submit_events_device: null array or bad count");
+    if (c->run_pending) {
+        const fd2_status w = fd2_wait(c);
+        if (w != FD2_OK) return w;
+    }
+    if (c->geoms.size() != 1) return fail(c, FD2_ERR_STATE, "cm submission is for a single geometry; use fd2_submit_events_um");
+    if (c->opt.count_mode == FD2_COUNT_GIVEN) return fail(c, FD2_ERR_STATE, "count_mode GIVEN needs fd2_submit_events_um");
+    FD2_CUDA(c, cudaSetDevice(c->device));
+    if (n > 0)
+        for (const void *p : {(const void *)x_cm, (const void *)y_cm, (const void *)z_cm, (const void *)de_ev,
+                              (const void *)hist}) {
+            cudaPointerAttributes at{};
+            if (cudaPointerGetAttributes(&at, p) != cudaSuccess ||
+                (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != c->device) {
+                cudaGetLastError();
+                return fail(c, FD2_ERR_INVALID_ARGUMENT, "submit_events_device: an array is not device memory of the context's GPU");
+            }
+        }
+    fd2_status st = ensure_events(c, n);
+    if (st != FD2_OK) return st;
+    FD2_CUDA(c, fd2::launch_prep_cm(c->stream, n, x_cm, y_cm, z_cm, de_ev, hist, c->n_prim, c->d_ev_pos, c->d_ev_e,
+                                    c->d_ev_xyz, c->d_flags));
+    c->has_geom = false;
+    // sums of x, y (um, as the host path rounds them) and of the energies
+    double sums[3] = {0, 0, 0};
+    if (n > 0) {
+        double *d_sums = nullptr;
+        FD2_CUDA(c, cudaMallocAsync((void **)&d_sums, 3 * sizeof(double), c->stream));
+        FD2_CUDA(c, cudaMemsetAsync(d_sums, 0, 3 * sizeof(double), c->stream));
+        FD2_CUDA(c, fd2::launch_event_sums(c->stream, n, x_cm, y_cm, de_ev, d_sums));
+        FD2_CUDA(c, cudaMemcpyAsync(sums, d_sums, sizeof sums, cudaMemcpyDeviceToHost, c->stream));
+        FD2_CUDA(c, cudaFreeAsync(d_sums, c->stream));
+        FD2_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    c->mu_total = sums[2] * c->params.yield;
+    return submit_common(c, n, nullptr, nullptr, nullptr, sums);
 }
 
 fd2_status fd2_submit_events_um(fd2_ctx *c, const float *x_um, const float *y_um, const float *z_um, const float *e_ev,

@@ -82,6 +82,10 @@ cudaError_t launch_count(cudaStream_t s, int64_t n, int64_t event_base, int mode
 cudaError_t launch_scan(cudaStream_t s, int64_t n, const uint32_t *in, unsigned long long *offsets,
                         unsigned long long *block_sums, unsigned long long *total);
 size_t scan_block_sums_needed(int64_t n);
+// Device-submitted events (fd2_xray.cu): out[0] += sum of (float)(x_cm 1e4),
+// out[1] the same for y, out[2] += sum of the positive energies.
+cudaError_t launch_event_sums(cudaStream_t s, int64_t n, const double *x_cm, const double *y_cm, const double *de,
+                              double *out);
 cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32_t *ev_n,
                                const unsigned long long *offsets, uint2 *chunks, int64_t capacity,
                                int *status);

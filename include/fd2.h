@@ -200,6 +200,14 @@ FD2_API fd2_status fd2_submit_events_um(fd2_ctx *ctx, const float *x_um, const f
                                         const float *z_um, const float *e_ev,
                                         const int32_t *hist, const int32_t *nphot,
                                         const uint16_t *geom, int64_t n);
+/* fd2_submit_events with the arrays in device memory of the context's
+ * device (a GPU producer such as the x-ray front end, fd2_xray.h): the
+ * events never pass through the host, and the transport is identical to a
+ * host submission of the same arrays.  The arrays must be complete when
+ * this is called (their producer synchronised); they are not kept. */
+FD2_API fd2_status fd2_submit_events_device(fd2_ctx *ctx, const double *x_cm, const double *y_cm,
+                                            const double *z_cm, const double *de_ev,
+                                            const int32_t *hist, int64_t n);
 
 /* Transport the resident events; tallies accumulate across runs.  Returns
  * once the work is queued on the context's stream. */
