@@ -21,6 +21,10 @@ photon counts ~ Poisson(E * 54/keV) sampled on the GPU each step.
           the same 1,000,000-x-ray, 500 um stream, with the PHS/Swank and PRF
           errors between the two and the same errors between two Monte Carlo
           runs (the noise floor)
+  xray_frontend  x-rays/s of the GPU x-ray front end (EDEs from x-rays by
+          FP64 photon + electron transport) on config 1's detector and
+          spectrum, alone and chained with the optical transport through the
+          device handoff
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU: one rank per GPU (torchrun); each rank transports its own x-ray
@@ -83,6 +87,7 @@ def parse():
     ap.add_argument("--surrogate-model", default=os.path.join(ROOT, "hybridmantis_b200", "data", "surrogate_c4.fd2sg"))
     ap.add_argument("--surrogate-xrays", type=int, default=1_000_000)
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-frontend", action="store_true")
     return ap.parse_args()
 
 
@@ -253,6 +258,47 @@ def _peaks():
         return {}
 
 
+def frontend_leg(params, device, seed, runs=3):
+    """The GPU x-ray front end on config 1's detector and spectrum: x-rays/s of
+    the front end alone (its kernels' CUDA-event times) and of the chain
+    x-ray -> EDEs -> device handoff -> optical transport -> tallies."""
+    import copy
+    import hybridmantis_b200 as hb
+    from hybridmantis_b200 import xray
+    p = copy.copy(params)
+    n = int(p.num_hist)
+    src = xray.triangular_spectrum(20e3, 40e3, 70e3, center_cm=(p.det_x * 0.5e-4, p.det_y * 0.5e-4, 1.0))
+    with xray.XrayFrontEnd(det_x_um=p.det_x, det_y_um=p.det_y, det_height_um=p.det_height, seed=seed,
+                           device=device) as fe, hb.OpticalTransport(p, device=device, seed=seed + 1) as t:
+        fe.run(src, n)  # warm-up (allocations)
+        fe.submit(t)
+        t.run_sync()
+        fe_ms, chain_ms, walls = [], [], []
+        for _ in range(runs):
+            t.reset_tallies()
+            w0 = time.perf_counter()
+            fe.run(src, n)
+            fe.submit(t)
+            t.run_sync()
+            walls.append(time.perf_counter() - w0)
+            ft = fe.timing()
+            fe_ms.append(ft["transport_ms"] + ft["compact_ms"])
+            chain_ms.append(fe_ms[-1] + t.timing()["pipeline_ms"])
+        st = fe.stats()
+        ps = t.phs_stats()
+        edes = fe.num_edes()
+        photons = t.timing()["photons"]
+    return {"metric": "x-rays/s", "value": n / (np.median(fe_ms) * 1e-3),
+            "chain_xrays_per_s": n / (np.median(chain_ms) * 1e-3),
+            "chain_wall_xrays_per_s": n / np.median(walls),
+            "workload": f"config-1 detector {p.det_x:g} x {p.det_y:g} x {p.det_height:g} um, {n} x-rays, "
+                        f"Triangular(20, 40, 70) keV pencil beam, FP64 photon + electron transport",
+            "frontend_ms": float(np.median(fe_ms)), "chain_ms": float(np.median(chain_ms)),
+            "edes_per_xray": edes / n, "photons_per_xray": photons / n,
+            "fluorescence_escape": st["fluorescence_escaped"] / max(st["fluorescence_emitted"], 1),
+            "phs_mean": ps["mean"], "swank": ps["swank"]}
+
+
 def run_ours(a, rank, world, local_rank):
     import torch
     import hybridmantis_b200 as hb
@@ -397,6 +443,9 @@ def run_ours(a, rank, world, local_rank):
                          "audit": {k: st[k] for k in ("audit_events", "audit_z", "audit_radial_l1", "audit_ms")},
                          "mc_fallback_events": st["mc_events"], "surrogate_events": st["surrogate_events"],
                          "model": os.path.relpath(a.surrogate_model, ROOT)}
+        frontend = None
+        if not a.no_frontend and world == 1:
+            frontend = frontend_leg(es.params, local_rank, a.seed)
         clocks = clk.summary()
         out = {
             "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": a.steps,
@@ -416,6 +465,7 @@ def run_ours(a, rank, world, local_rank):
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
             "surrogate": surrogate,
+            "xray_frontend": frontend,
             "clocks": clocks,
             "results": {"phs_mean": stats["mean"], "swank": stats["swank"],
                         "fates_per_photon": {k: cnt[k] / max(cnt["generated"], 1) for k in
