@@ -163,6 +163,9 @@ class CpuReference:
 # of the config-1 stream, 2,000 x-rays); the traffic is one event record per
 # chunk and grows in proportion to the photons.
 TRANSPORT_DRAM_BYTES_PER_PHOTON = 3338240.0 / 4690971.0
+# Issue slots the transport kernel uses in steady state (ncu
+# smsp__issue_active of 20,000 config-1 x-rays, where its tail is small).
+TRANSPORT_ISSUE_ACTIVE = 0.554
 
 
 def reference_gpu(es, nphot, device):
@@ -288,7 +291,16 @@ def frontend_leg(params, device, seed, runs=3):
         ps = t.phs_stats()
         edes = fe.num_edes()
         photons = t.timing()["photons"]
+    # CPU baseline: the same model restated in C (the front end's oracle), one core, a bounded sample
+    from oracle import xray_oracle as xo
+    m = 20000
+    w0 = time.perf_counter()
+    xo.run(xray.CSI_TABLE, src, m, det_x_um=p.det_x, det_y_um=p.det_y, det_height_um=p.det_height, seed=seed)
+    cpu_dt = time.perf_counter() - w0
     return {"metric": "x-rays/s", "value": n / (np.median(fe_ms) * 1e-3),
+            "cpu_baseline": {"value": m / cpu_dt, "unit": "x-rays/s", "cores": 1, "kind": "port",
+                             "sample": f"{m} histories of the same source, oracle/xray_oracle.c (gcc -O2, FP64), "
+                                       f"{cpu_dt:.1f} s"},
             "chain_xrays_per_s": n / (np.median(chain_ms) * 1e-3),
             "chain_wall_xrays_per_s": n / np.median(walls),
             "workload": f"config-1 detector {p.det_x:g} x {p.det_y:g} x {p.det_height:g} um, {n} x-rays, "
@@ -415,7 +427,12 @@ def run_ours(a, rank, world, local_rank):
                     "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 (FMA) x {sm_max:.0f} MHz "
                                    f"(sm_max_mhz of MEASURED_PEAKS.json; the file has no FP32 entry)",
                     "work_per_photon_fp32_ops": wpp, "kernel_ms_per_launch": avg_kern_s * 1e3,
-                    "photons_per_launch": photons_per_launch}
+                    "photons_per_launch": photons_per_launch,
+                    # the north-star criterion for this issue-bound kernel: scheduler issue slots used
+                    "issue_slot_utilisation": TRANSPORT_ISSUE_ACTIVE,
+                    "issue_slot_source": "ncu smsp__issue_active.avg.pct_of_peak_sustained_active of the same "
+                                         "kernel on 20,000 config-1 x-rays (steady state, "
+                                         "profiles/transport_kernel_config1_20k.md)"}
         cpu = None
         if not a.no_cpu_baseline and world == 1:
             ref = CpuReference(es, nphot)
