@@ -683,6 +683,7 @@ static fd2_status submit_common(fd2_ctx *c, int64_t n, const float *xs, const fl
                                 const double *sums = nullptr)
 {
     c->n_events = n;
+    c->submitted = true;
     c->counts_ready = false;
     c->graph_valid = false;
     c->ran_once = false;
@@ -869,8 +870,19 @@ fd2_status fd2_run(fd2_ctx *c)
 {
     if (c && c->ingest_active) return fail(c, FD2_ERR_STATE, "an event ingest is open; end it first");
     if (!c) return FD2_ERR_INVALID_ARGUMENT;
-    if (c->n_events <= 0 && !c->ran_once && c->cap_events == 0) return fail(c, FD2_ERR_STATE, "no events submitted");
+    if (c->n_events <= 0 && !c->ran_once && c->cap_events == 0 && !c->submitted)
+        return fail(c, FD2_ERR_STATE, "no events submitted");
     FD2_CUDA(c, cudaSetDevice(c->device));
+    if (c->n_events <= 0) {
+        // an empty submission: nothing to transport, tallies unchanged
+        FD2_CUDA(c, cudaMemsetAsync(c->d_scalars + 3, 0, sizeof(unsigned long long) * c->geoms.size(), c->stream));
+        cudaEvent_t marks[4] = {c->ev_start, c->ev_t0, c->ev_t1, c->ev_end};
+        for (cudaEvent_t e : marks) FD2_CUDA(c, cudaEventRecord(e, c->stream));
+        c->run_pending = true;
+        c->counts_ready = true;
+        c->ran_once = true;
+        return FD2_OK;
+    }
     fd2_status st = ensure_chunks(c);
     if (st != FD2_OK) return st;
     *c->h_abort = 0;

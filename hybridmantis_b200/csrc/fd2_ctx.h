@@ -67,6 +67,7 @@ struct fd2_ctx {
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     bool graph_valid = false;
     bool run_pending = false, ran_once = false;
+    bool submitted = false;  // a submission (possibly of zero events) happened
     bool ingest_active = false;  // fd2_ingest_begin .. fd2_ingest_end
     fd2_ingest *ingest = nullptr; // the open ingest, ended by fd2_destroy
     fd2::TransportConfig cfg;

@@ -210,6 +210,22 @@ def test_too_many_photons(require_gpu):
         assert ei.value.status == 6
 
 
+def test_empty_submission(require_gpu):
+    # an empty EDE buffer is a valid submission: the run transports nothing and leaves the tallies alone
+    p = hb.default_params(num_hist=4)
+    with hb.OpticalTransport(p) as t:
+        e = np.zeros(0)
+        t.submit_events(e, e, e, e, np.zeros(0, np.int32))
+        t.run_sync()
+        c = t.counters()
+        assert c["generated"] == 0 and c["detected"] == 0
+        assert t.phs().sum() == 0 and t.prf().sum() == 0 and t.timing()["photons"] == 0
+        v = np.full(3, 0.025)
+        t.submit_events(v, v, np.zeros(3), np.full(3, 1e4), np.array([1, 2, 3], np.int32))
+        t.run_sync()
+        assert t.counters()["generated"] > 0
+
+
 def test_deadline_aborts_and_context_recovers(require_gpu):
     es = hb.synth_events(1, 4000, 3)
     with hb.OpticalTransport(es.params, wait_timeout_s=1e-6) as t:

@@ -147,3 +147,50 @@ def test_device_submission_rejects_host_arrays(require_gpu):
         from hybridmantis_b200._lib import ptr
         st = lib.fd2_submit_events_device(t._h, ptr(x), ptr(x), ptr(np.zeros(4)), ptr(np.full(4, 1e4)), ptr(h), 4)
         assert st == 1
+
+
+def test_source_that_misses_the_slab(require_gpu):
+    # aimed away from the slab: no EDEs; the empty stream still goes through the handoff
+    src = xray.monoenergetic(30e3, direction=(0.0, 0.0, 1.0))
+    p = hb.default_params()
+    p.num_hist = 100
+    with xray.XrayFrontEnd(det_x_um=p.det_x, det_y_um=p.det_y, det_height_um=p.det_height) as fe:
+        fe.run(src, 100)
+        assert fe.num_edes() == 0
+        st = fe.stats()
+        assert st["missed"] == 100 and st["e_escaped_photon_ev"] == pytest.approx(100 * 30e3)
+        info = fe.history_info()
+        assert np.all(info["first_kind"] == 0) and np.all(info["first_depth_cm"] == -1.0)
+        with hb.OpticalTransport(p) as t:
+            fe.submit(t)
+            t.run_sync()
+            assert t.counters()["generated"] == 0
+
+
+def test_full_history_slots_merge_like_the_oracle(require_gpu):
+    # 64 slots and every electron tracked to 50 eV: long histories add the rest to their last EDE
+    src = xray.monoenergetic(70e3)
+    n = 1500
+    with xray.XrayFrontEnd(seed=9, electron_local_ev=50.0, max_edes_per_history=64) as fe:
+        fe.run(src, n)
+        info, g_edes, _ = gpu_edes(fe)
+        st = fe.stats()
+    h, o_edes = xo.run(xray.CSI_TABLE, src, n, seed=9, local_e=50.0, cap=64)
+    assert st["merged_histories"] > 0 and st["merged_histories"] == int(h["merged"].sum())
+    same = sum(a.shape == b.shape and (a.size == 0 or (np.abs(a - b).max() < 1e-6)) for a, b in zip(g_edes, o_edes))
+    assert same / n >= 0.99
+    assert int(info["n_edes"].max()) == 64
+    bal = np.array([e[:, 3].sum() for e in g_edes]) + info["e_escaped_photon_ev"] + \
+        info["e_escaped_electron_ev"] - info["e_source_ev"]
+    assert np.abs(bal).max() < 1e-6
+
+
+def test_invalid_sources_are_refused(require_gpu):
+    with xray.XrayFrontEnd() as fe:
+        for bad in (xray.Source(np.array([30e3, 20e3]), np.array([1.0, -1.0])),       # decreasing energies
+                    xray.Source(np.array([30e3, 40e3, 50e3]), np.array([0.0, 0.0, -1.0])),  # no probability
+                    xray.monoenergetic(30e3, semiaperture_deg=200.0),
+                    xray.monoenergetic(30e3, direction=(0.0, 0.0, 0.0))):
+            with pytest.raises(hb.Fd2Error) as e:
+                fe.run(bad, 10)
+            assert e.value.status == 1
