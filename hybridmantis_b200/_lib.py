@@ -191,7 +191,7 @@ EXPORTED = [
     "fd2_xray_attenuation", "fd2_xray_electron_tables", "fd2_xray_default_options", "fd2_xray_create",
     "fd2_xray_destroy", "fd2_xray_last_error", "fd2_xray_run", "fd2_xray_num_edes", "fd2_xray_get_edes",
     "fd2_xray_get_history_info", "fd2_xray_get_stats", "fd2_xray_clear_stats", "fd2_xray_get_timing",
-    "fd2_xray_submit", "fd2_xray_device_edes", "fd2_xray_sample",
+    "fd2_xray_submit", "fd2_xray_device_edes", "fd2_xray_sample", "fd2_xray_read_penEasy_source",
 ]
 
 
@@ -296,6 +296,7 @@ def load():
         "fd2_xray_device_edes": (ctypes.c_int, [vp, P(vp), P(vp), P(vp), P(vp), P(vp), P(ctypes.c_int64)]),
         "fd2_xray_sample": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
                                            ctypes.c_uint64, vp]),
+        "fd2_xray_read_penEasy_source": (ctypes.c_int, [ctypes.c_char_p, P(XraySource), vp, vp, ctypes.c_int32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

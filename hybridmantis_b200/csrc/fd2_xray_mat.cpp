@@ -559,3 +559,52 @@ void electron_at(const Material &m, double E, double *range, double *lambda1)
 }
 
 }  // namespace fd2x
+
+extern "C" FD2_API fd2_status fd2_xray_read_penEasy_source(const char *path, fd2_xray_source *src, double *e_ev,
+                                                           double *prob, int32_t cap)
+{
+    if (!path || !src || !e_ev || !prob || cap < 2) return FD2_ERR_INVALID_ARGUMENT;
+    std::ifstream f(path);
+    if (!f) return FD2_ERR_IO;
+    std::string line;
+    bool found = false;
+    while (std::getline(f, line))
+        if (line.find("[SECTION SOURCE BOX ISOTROPIC GAUSS SPECTRUM") != std::string::npos) {
+            found = true;
+            break;
+        }
+    if (!found || !std::getline(f, line)) return FD2_ERR_PARSE;
+    // status field "(ON )": the three characters after the first
+    const std::string st = line.size() >= 4 ? line.substr(1, 3) : "";
+    if (st.find("ON") == std::string::npos) return FD2_ERR_PARSE;
+    auto nums = [&](int k, double *v) {
+        if (!std::getline(f, line)) return false;
+        std::istringstream is(line);
+        for (int i = 0; i < k; ++i)
+            if (!(is >> v[i])) return false;
+        return true;
+    };
+    double v[3];
+    if (!nums(1, v)) return FD2_ERR_PARSE;
+    fd2_xray_source s{};
+    s.particle = (int32_t)v[0];
+    if (!std::getline(f, line)) return FD2_ERR_PARSE;  // the spectrum's title line
+    int n = 0;
+    for (;;) {
+        if (!nums(2, v) || n >= cap) return FD2_ERR_PARSE;
+        e_ev[n] = v[0];
+        prob[n] = v[1];
+        ++n;
+        if (v[1] < 0.0) break;
+    }
+    s.n_spectrum = n;
+    s.e_ev = e_ev;
+    s.prob = prob;
+    if (!nums(3, s.center_cm) || !nums(3, s.sides_cm) || !nums(3, s.euler_deg)) return FD2_ERR_PARSE;
+    if (!nums(1, v) || v[0] != 0.0) return FD2_ERR_PARSE;  // source material: only 0 (any) is supported
+    if (!nums(3, s.direction) || !nums(1, v)) return FD2_ERR_PARSE;
+    s.semiaperture_deg = v[0];
+    *src = s;
+    return FD2_OK;
+}
+

@@ -117,31 +117,17 @@ def triangular_spectrum(lo_ev: float, mode_ev: float, hi_ev: float, bins: int = 
 
 
 def read_penEasy_source(path: str) -> Source:
-    """The BIGS section of a penEasy input file (sourceBoxIsotropicGaussSpectrum.f:218-400)."""
-    lines = open(path).read().splitlines()
-    head = "[SECTION SOURCE BOX ISOTROPIC GAUSS SPECTRUM"
-    i = next(k for k, s in enumerate(lines) if s.startswith(head))
-    status = lines[i + 1].strip()
-    if not status.startswith("(ON"):
-        raise ValueError("the BIGS source is OFF in " + path)
-    particle = int(lines[i + 2].split()[0])
-    k = i + 4  # after the 'Energy(eV) Probability' title line
-    e, p = [], []
-    while True:
-        a, b = lines[k].split()[:2]
-        e.append(float(a))
-        p.append(float(b))
-        k += 1
-        if float(b) < 0:
-            break
-    nums = [[float(v) for v in lines[k + j].split()[:3]] for j in range(3)]
-    mat = int(lines[k + 3].split()[0])
-    direction = [float(v) for v in lines[k + 4].split()[:3]]
-    aperture = float(lines[k + 5].split()[0])
-    if mat != 0:
-        raise ValueError("only MATERIAL 0 (any material) sources are supported")
-    return Source(np.array(e), np.array(p), particle=particle, center_cm=tuple(nums[0]), sides_cm=tuple(nums[1]),
-                  euler_deg=tuple(nums[2]), direction=tuple(direction), semiaperture_deg=aperture)
+    """The BIGS section of a penEasy input file (fd2_xray_read_penEasy_source)."""
+    cap = 100000
+    e = np.zeros(cap)
+    pr = np.zeros(cap)
+    s = XraySource()
+    check(load().fd2_xray_read_penEasy_source(path.encode(), ctypes.byref(s), ptr(e), ptr(pr), cap),
+          f"read_penEasy_source({path})")
+    n = s.n_spectrum
+    return Source(e[:n].copy(), pr[:n].copy(), particle=s.particle, center_cm=tuple(s.center_cm),
+                  sides_cm=tuple(s.sides_cm), euler_deg=tuple(s.euler_deg), direction=tuple(s.direction),
+                  semiaperture_deg=s.semiaperture_deg)
 
 
 class XrayFrontEnd:

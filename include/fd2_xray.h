@@ -109,6 +109,14 @@ typedef struct fd2_xray_source {
     double semiaperture_deg;        /* cone half-angle, [0, 180] */
 } fd2_xray_source;
 
+/* Read the SOURCE BOX ISOTROPIC GAUSS SPECTRUM section of a penEasy input
+ * file (read in the order of sourceBoxIsotropicGaussSpectrum.f:218-400):
+ * fills *src and copies the spectrum lines into e_ev / prob (cap lines at
+ * most; src->e_ev / src->prob point at them).  FD2_ERR_PARSE if the section
+ * is missing or OFF, or names a source material other than 0. */
+FD2_API fd2_status fd2_xray_read_penEasy_source(const char *path, fd2_xray_source *src, double *e_ev, double *prob,
+                                                int32_t cap);
+
 typedef struct fd2_xray_options {
     int32_t device;
     double det_x_um, det_y_um;      /* slab: x in (0, det_x), y in (0, det_y) */

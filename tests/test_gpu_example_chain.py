@@ -76,3 +76,46 @@ def test_reference_example_end_to_end(require_gpu):
     dof = int((ref_phs + phs > 0).sum()) - 1
     assert chi2 < dof + 6 * np.sqrt(2 * dof), rep
     assert rep["prf_l1"] < 0.03, rep
+
+
+BIGS = """[SECTION SOURCE BOX ISOTROPIC GAUSS SPECTRUM v.2006-08-01]
+(ON )                            STATUS (ON or OFF)
+ 2                               PARTICLE TYPE (1=electron, 2=photon, 3=positron)
+ Energy(eV)  Probability         ENERGY SPECTRUM
+ 25.0e3       1.0
+ 25.0e3       0.000000010
+  1.e6        -1
+ 4.540e-2  4.540e-2  1.000e0     CENTER COORDINATES OF THE BOX ENCLOSURE (cm)
+ 3.000e-3  3.000e-3  0.000e0     BOX SIDES (cm)
+ 0.000e0  0.000e0  0.000e0       EULER ANGLES [Rz,Ry,Rz](deg) TO ROTATE BOX
+ 0                               MATERIAL (0=DO NOT CARE)
+ 0.000e0  0.000e0  -1.000        DIRECTION VECTOR, NO NEED TO NORMALIZE
+ 0.000e0                         ANGLE OF SEMIAPERTURE [0,180] (deg)
+[END OF BIGS SECTION]
+"""
+
+
+def test_fd2run_runs_the_example_from_its_input_files(require_gpu, tmp_path):
+    """The command-line driver, x-ray mode: a penEasy source section (the example's, with its 1e-8
+    tail bin up to 1 MeV), the CsI tables and hybridMANTIS_input.in in; the reference's two output
+    files out, under the reference's own file names."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "hybridmantis_b200", "bin", "fd2run")
+    pe = tmp_path / "penEasy.in"
+    pe.write_text("# penEasy input (source section only)\n" + BIGS)
+    out = tmp_path / "out"
+    out.mkdir()
+    r = subprocess.run([exe, "--seed", "11", "--xray", str(pe), "--material", xray.CSI_TABLE, "--out", str(out),
+                        os.path.join(GOLDEN, "example_hybridMANTIS_input.in")], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    z = np.load(os.path.join(GOLDEN, "example_myimage.npz"))
+    names = sorted(os.listdir(out))
+    assert names == sorted([str(z["detected_name"]), str(z["name"])]), names
+    phs = np.array([float(v) for v in open(out / str(z["detected_name"]))])
+    ref_phs = np.array([float(v) for v in open(os.path.join(GOLDEN, "example_detected.txt"))])
+    _, gmean, gswank = phs_stats(phs)
+    _, rmean, rswank = phs_stats(ref_phs)
+    assert gmean == pytest.approx(rmean, rel=0.01) and gswank == pytest.approx(rswank, abs=0.003), r.stdout
+    assert "Depositions per primary" in r.stdout

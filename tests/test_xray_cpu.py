@@ -163,6 +163,22 @@ def test_penEasy_source_section(tmp_path):
     assert s.euler_deg == (0.0, 10.0, 0.0) and s.direction == (0.0, 0.0, -1.0) and s.semiaperture_deg == 2.5
 
 
+def test_penEasy_source_section_refusals(tmp_path):
+    good = (tmp_path / "g.in")
+    base = [" 2   PARTICLE", " Energy(eV)  Probability", " 30.0e3 1.0", " 30.0e3 -1", " 0.04 0.04 1.0", " 0 0 0",
+            " 0 0 0", " 0", " 0 0 -1", " 0.0"]
+    head = "[SECTION SOURCE BOX ISOTROPIC GAUSS SPECTRUM v.2006-08-01]"
+    good.write_text("\n".join([head, "(ON )"] + base) + "\n")
+    assert xray.read_penEasy_source(str(good)).e_ev.tolist() == [30e3, 30e3]
+    for name, lines in (("off", [head, "(OFF)"] + base), ("mat", [head, "(ON )"] + base[:7] + [" 1"] + base[8:]),
+                        ("none", ["[SECTION SOURCE PHASE SPACE FILE v.2008-06-01]", "(ON )"])):
+        f = tmp_path / f"{name}.in"
+        f.write_text("\n".join(lines) + "\n")
+        with pytest.raises(hb.Fd2Error) as e:
+            xray.read_penEasy_source(str(f))
+        assert e.value.status == 3
+
+
 # ------------------------------------------------------------------ oracle
 
 def run(src, n, **kw):
