@@ -60,3 +60,29 @@ def test_reference_cuda_kernel_statistics(require_gpu, ref_cuda):
     assert abs(z_mean) < 5.0, rep
     assert abs(z_swank) < 5.0, rep
     assert chi2 < dof + 6 * np.sqrt(2 * dof), rep
+
+
+def test_reference_generated_counter_counts_zero_photon_events(require_gpu, ref_cuda):
+    """The reference kernel counts the first photon of every event before its loop
+    (main/kernel_cuda_c_ver1_0.cu:443), so each event with N = 0 adds one "generated" photon
+    that is never transported: its console's generated total exceeds the sum of its fate
+    counters by the number of zero-photon EDEs (12.0 M of the example run's 95.2 M).  This
+    library counts the photons it transports."""
+    es, N = c0_events(300, seed=8)
+    N = N.copy()
+    N[::3] = 0
+    p = es.params
+    ref = ref_cuda.run_ref_cuda(oracle_geometry(p), es.x_um.astype(np.float64), es.y_um.astype(np.float64),
+                                es.z_um.astype(np.float64), es.hist, N, num_hist=p.num_hist)
+    rc = dict(zip(po.COUNTER_NAMES, [int(v) for v in ref.counters]))
+    n, zeros = int(N.sum()), int((N == 0).sum())
+    fates = rc["detect"] + rc["abs_top"] + rc["abs_bulk"] + rc["lost"] + rc["outofcol"] + rc["theta1"]
+    report("reference_generated_counter", {"ref": rc, "photons": n, "zero_events": zeros, "ref_fate_sum": fates})
+    assert rc["generated"] == n + zeros
+    assert abs(fates - n) <= 1e-3 * n
+    with hb.OpticalTransport(p, count_mode=hb.COUNT_GIVEN, seed=3) as t:
+        t.submit(es, nphot=N)
+        t.run_sync()
+        c = t.counters()
+    assert c["generated"] == n
+    assert sum(c[k] for k in ("detected", "abs_top", "abs_bulk", "lost", "outofcol", "theta1", "capped")) == n
