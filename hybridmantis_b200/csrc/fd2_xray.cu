@@ -744,12 +744,12 @@ struct fd2_xray {
     XDev dev{};
     // batch buffers
     Ede *d_slots = nullptr;
-    HistInfo *d_info_batch = nullptr;
+    HistInfo *d_info = nullptr;  // the run's per-history records (device; copied out on request)
+    int64_t info_cap = 0, n_info = 0;
     uint32_t *d_counts = nullptr;
     unsigned long long *d_offsets = nullptr, *d_block_sums = nullptr, *d_total = nullptr;
     int64_t batch_cap = 0;
     // run outputs
-    std::vector<HistInfo> info;  // host copy of the last run's per-history records
     double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr, *d_de = nullptr;
     int32_t *d_hist = nullptr;
     int64_t out_cap = 0, n_out = 0;
@@ -883,13 +883,11 @@ fd2_status ensure_batch(fd2_xray *x, int64_t b)
 {
     if (b <= x->batch_cap) return FD2_OK;
     dfree(x->d_slots);
-    dfree(x->d_info_batch);
     dfree(x->d_counts);
     dfree(x->d_offsets);
     dfree(x->d_block_sums);
     x->batch_cap = 0;
     XCUDA(x, cudaMalloc(&x->d_slots, sizeof(Ede) * (size_t)b * x->opt.max_edes_per_history));
-    XCUDA(x, cudaMalloc(&x->d_info_batch, sizeof(HistInfo) * (size_t)b));
     XCUDA(x, cudaMalloc(&x->d_counts, sizeof(uint32_t) * (size_t)b));
     XCUDA(x, cudaMalloc(&x->d_offsets, sizeof(unsigned long long) * (size_t)b));
     XCUDA(x, cudaMalloc(&x->d_block_sums, sizeof(unsigned long long) * std::max<size_t>(fd2::scan_block_sums_needed(b), 1)));
@@ -1144,7 +1142,7 @@ FD2_API void fd2_xray_destroy(fd2_xray *x)
     for (double *p : {x->d_e, x->d_lnv, x->d_ee, x->d_lnee, x->d_lnr, x->d_lnl1, x->d_bind, x->d_tcum, x->d_te, x->d_x,
                       x->d_y, x->d_z, x->d_de, x->d_spec})
         if (p) cudaFree(p);
-    for (void *p : {(void *)x->d_toff, (void *)x->d_ts, (void *)x->d_slots, (void *)x->d_info_batch,
+    for (void *p : {(void *)x->d_toff, (void *)x->d_ts, (void *)x->d_slots, (void *)x->d_info,
                     (void *)x->d_counts, (void *)x->d_offsets, (void *)x->d_block_sums, (void *)x->d_total,
                     (void *)x->d_hist, (void *)x->d_tot})
         if (p) cudaFree(p);
@@ -1167,17 +1165,24 @@ FD2_API fd2_status fd2_xray_run(fd2_xray *x, const fd2_xray_source *src, int64_t
     if (st != FD2_OK) return st;
     const int64_t B = std::min<int64_t>(x->opt.batch_histories, std::max<int64_t>(n, 1));
     if ((st = ensure_batch(x, B)) != FD2_OK) return st;
-    x->info.resize((size_t)n);
+    if (n > x->info_cap) {
+        dfree(x->d_info);
+        x->info_cap = 0;
+        XCUDA(x, cudaMalloc(&x->d_info, sizeof(HistInfo) * (size_t)std::max<int64_t>(n, 1)));
+        x->info_cap = n;
+    }
+    x->n_info = n;
     x->n_out = 0;
     x->t_transport = x->t_compact = 0;
     for (int64_t b0 = 0; b0 < n; b0 += B) {
         const int64_t nb = std::min(B, n - b0);
         const unsigned grid = (unsigned)((nb + 127) / 128);
         XCUDA(x, cudaEventRecord(x->ev[0], x->stream));
-        history_kernel<<<grid, 128, 0, x->stream>>>(x->dev, s, first + b0, nb, x->d_slots, x->d_info_batch);
+        HistInfo *info = x->d_info + b0;
+        history_kernel<<<grid, 128, 0, x->stream>>>(x->dev, s, first + b0, nb, x->d_slots, info);
         XCUDA(x, cudaGetLastError());
         XCUDA(x, cudaEventRecord(x->ev[1], x->stream));
-        count_kernel<<<grid, 128, 0, x->stream>>>(x->d_info_batch, nb, x->d_counts);
+        count_kernel<<<grid, 128, 0, x->stream>>>(info, nb, x->d_counts);
         XCUDA(x, cudaGetLastError());
         XCUDA(x, fd2::launch_scan(x->stream, nb, x->d_counts, x->d_offsets, x->d_block_sums, x->d_total));
         unsigned long long tot = 0;
@@ -1185,13 +1190,11 @@ FD2_API fd2_status fd2_xray_run(fd2_xray *x, const fd2_xray_source *src, int64_t
         XCUDA(x, cudaStreamSynchronize(x->stream));
         if ((st = ensure_out(x, x->n_out + (int64_t)tot)) != FD2_OK) return st;
         XCUDA(x, cudaEventRecord(x->ev[2], x->stream));
-        scatter_kernel<<<grid, 128, 0, x->stream>>>(x->d_info_batch, x->d_slots, x->opt.max_edes_per_history, nb,
+        scatter_kernel<<<grid, 128, 0, x->stream>>>(info, x->d_slots, x->opt.max_edes_per_history, nb,
                                                    first + b0, x->d_offsets, x->n_out, x->d_x, x->d_y, x->d_z,
                                                    x->d_de, x->d_hist, x->d_tot);
         XCUDA(x, cudaGetLastError());
         XCUDA(x, cudaEventRecord(x->ev[3], x->stream));
-        XCUDA(x, cudaMemcpyAsync(x->info.data() + b0, x->d_info_batch, sizeof(HistInfo) * nb,
-                                 cudaMemcpyDeviceToHost, x->stream));
         XCUDA(x, cudaStreamSynchronize(x->stream));
         float a = 0, c = 0, d = 0;
         cudaEventElapsedTime(&a, x->ev[0], x->ev[1]);
@@ -1232,9 +1235,14 @@ FD2_API fd2_status fd2_xray_get_history_info(fd2_xray *x, double *e0, double *es
                                              int32_t *kind, int32_t *nedes, int64_t n)
 {
     if (!x || n < 0) return FD2_ERR_INVALID_ARGUMENT;
-    if (n > (int64_t)x->info.size()) return xfail(x, FD2_ERR_INVALID_ARGUMENT, "history_info: n above the run's histories");
+    if (n > x->n_info) return xfail(x, FD2_ERR_INVALID_ARGUMENT, "history_info: n above the run's histories");
+    std::vector<HistInfo> info((size_t)n);
+    if (n) {
+        XCUDA(x, cudaSetDevice(x->device));
+        XCUDA(x, cudaMemcpy(info.data(), x->d_info, sizeof(HistInfo) * (size_t)n, cudaMemcpyDeviceToHost));
+    }
     for (int64_t i = 0; i < n; ++i) {
-        const HistInfo &h = x->info[(size_t)i];
+        const HistInfo &h = info[(size_t)i];
         if (e0) e0[i] = h.e0;
         if (esc_ph) esc_ph[i] = h.esc_ph;
         if (esc_el) esc_el[i] = h.esc_el;
