@@ -9,3 +9,4 @@ from .fastdetect2 import (COUNT_GAUSSIAN, COUNT_GIVEN, COUNT_POISSON, REPLAY_FP6
                           read_events_binary, read_events_text, read_input_file, synth_events,
                           write_events_binary, write_events_text, write_output_files)
 from .surrogate import Surrogate  # noqa: F401,E402
+from .xray import Material as XrayMaterial, XrayFrontEnd  # noqa: F401,E402

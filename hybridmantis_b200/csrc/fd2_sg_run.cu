@@ -390,8 +390,11 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
     if (cudaSetDevice(c->device) != cudaSuccess) return sg_fail(s, FD2_ERR_CUDA, "set device");
     if ((st = fd2::api::ensure_chunks(c)) != FD2_OK) return sg_fail(s, st, "context chunks");
     const int64_t n = c->n_events;
-    // the network's GEMM grid has one row of CTAs per 64 events
-    if (n > (int64_t)65535 * kBM) return sg_fail(s, FD2_ERR_INVALID_ARGUMENT, "more than 4,194,240 events per run");
+    // the tensor-core forward is persistent; the mma.sync one (FD2_SG_GEMM=mma) has one grid row of CTAs
+    // per 64 events
+    if (!s->use_tc && n > (int64_t)65535 * kBM)
+        return sg_fail(s, FD2_ERR_INVALID_ARGUMENT, "more than 4,194,240 events per run on the mma.sync forward");
+    if (n >= ((int64_t)1 << 31)) return sg_fail(s, FD2_ERR_INVALID_ARGUMENT, "2^31 events or more per run");
     if ((st = ensure_run_buffers(s, n)) != FD2_OK) return st;
     RunBuffers *R = s->run;
     cudaStream_t q = c->stream;

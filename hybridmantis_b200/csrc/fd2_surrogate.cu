@@ -359,7 +359,10 @@ static cudaError_t sg_dense(fd2_sg *s, cudaStream_t st, const GemmArgs &g)
 {
     const bool tc = s->use_tc && g.K % 16 == 0 && g.K <= kTcMaxK && g.N % 16 == 0 && g.N >= 16 && g.N <= kTcMaxN &&
                     g.lda % 8 == 0 && g.ldb % 8 == 0 && g.ldc % 16 == 0 && g.M > 0;
-    if (!tc) return sg_gemm(st, true, true, g, 1);
+    if (!tc) {
+        if ((int64_t)g.M > (int64_t)65535 * kBM) return cudaErrorInvalidValue;  // one grid row per 64 rows
+        return sg_gemm(st, true, true, g, 1);
+    }
     TcArgs t;
     t.A = g.A;
     t.B = g.B;

@@ -35,9 +35,25 @@ def _radial(img, cx, cy, edges):
 
 
 def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 4242, audit: float = 0.01,
-             device: int = 0, repeats: int = 2, noise_floor: bool = False) -> dict:
-    es = fd.synth_events(config, xrays, seed)
-    out = {"config": config, "xrays": es.params.num_hist, "events": es.n}
+             device: int = 0, repeats: int = 2, noise_floor: bool = False, frontend: bool = False) -> dict:
+    """With ``frontend`` the events come from the GPU x-ray front end (the
+    configuration's detector and Triangular(20, 40, 70) keV pencil beam at its
+    centre) instead of the synthetic cluster generator, handed to each
+    context on the device."""
+    fe = None
+    if frontend:
+        from . import xray
+        es = fd.synth_events(config, 1, seed)
+        p = es.params
+        p.num_hist = xrays
+        fe = xray.XrayFrontEnd(det_x_um=p.det_x, det_y_um=p.det_y, det_height_um=p.det_height, seed=seed,
+                               device=device)
+        fe.run(xray.triangular_spectrum(20e3, 40e3, 70e3, center_cm=(p.det_x * 0.5e-4, p.det_y * 0.5e-4, 1.0)),
+               xrays)
+        out = {"config": config, "xrays": xrays, "events": fe.num_edes(), "events_from": "x-ray front end"}
+    else:
+        es = fd.synth_events(config, xrays, seed)
+        out = {"config": config, "xrays": es.params.num_hist, "events": es.n}
     res = {}
     with sgm.Surrogate(device=device) as s:
         s.load(model)
@@ -47,7 +63,10 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
             # mc2: the Monte Carlo again with other random streams (the
             # noise floor of the comparison)
             with fd.OpticalTransport(es.params, device=device, seed=seed + (2 if mode == "mc2" else 1)) as t:
-                t.submit(es)
+                if fe is not None:
+                    fe.submit(t)
+                else:
+                    t.submit(es)
                 # warm-up run, then timed runs on reset tallies
                 if mode != "sg":
                     t.run_sync()
@@ -67,11 +86,15 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
                 img = t.prf().astype(np.float64)
                 c = t.counters()
             mean, swank = _moments(prim)
-            res[mode] = {"seconds": min(times), "xrays_per_s": es.params.num_hist / min(times), "phs_mean": mean,
+            res[mode] = {"seconds": min(times), "xrays_per_s": out["xrays"] / min(times), "phs_mean": mean,
                          "swank": swank, "detected": c["detected"], "image": img, "stats": stats}
     edges = np.array([0, 1, 2, 3, 4, 6, 8, 11, 15, 20, 30, 45, 70, 110, 170, 260, 400])
-    cx = float(np.mean(es.x_um)) - es.params.lb_x
-    cy = float(np.mean(es.y_um)) - es.params.lb_y
+    if fe is not None:
+        cx, cy = 0.5 * es.params.det_x - es.params.lb_x, 0.5 * es.params.det_y - es.params.lb_y
+        fe.close()
+    else:
+        cx = float(np.mean(es.x_um)) - es.params.lb_x
+        cy = float(np.mean(es.y_um)) - es.params.lb_y
     rm, rs = _radial(res["mc"]["image"], cx, cy, edges), _radial(res["sg"]["image"], cx, cy, edges)
     im, isg = res["mc"]["image"], res["sg"]["image"]
     out.update({
@@ -106,8 +129,10 @@ def main():
     ap.add_argument("--seed", type=int, default=4242)
     ap.add_argument("--audit", type=float, default=0.01)
     ap.add_argument("--noise-floor", action="store_true")
+    ap.add_argument("--xray-frontend", action="store_true", help="events from the GPU x-ray front end")
     a = ap.parse_args()
-    print(json.dumps(evaluate(a.model, a.config, a.xrays, a.seed, a.audit, noise_floor=a.noise_floor)))
+    print(json.dumps(evaluate(a.model, a.config, a.xrays, a.seed, a.audit, noise_floor=a.noise_floor,
+                              frontend=a.xray_frontend)))
 
 
 if __name__ == "__main__":
