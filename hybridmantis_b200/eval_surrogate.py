@@ -35,7 +35,8 @@ def _radial(img, cx, cy, edges):
 
 
 def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 4242, audit: float = 0.01,
-             device: int = 0, repeats: int = 2, noise_floor: bool = False, frontend: bool = False) -> dict:
+             device: int = 0, repeats: int = 2, noise_floor: bool = False, frontend: bool = False,
+             lateral_um: float = 50.0) -> dict:
     """With ``frontend`` the events come from the GPU x-ray front end (the
     configuration's detector and Triangular(20, 40, 70) keV pencil beam at its
     centre) instead of the synthetic cluster generator, handed to each
@@ -55,7 +56,8 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
         es = fd.synth_events(config, xrays, seed)
         out = {"config": config, "xrays": es.params.num_hist, "events": es.n}
     res = {}
-    with sgm.Surrogate(device=device) as s:
+    out["lateral_um"] = lateral_um
+    with sgm.Surrogate(device=device, lateral_um=lateral_um) as s:
         s.load(model)
         for mode in ("mc", "mc2", "sg"):
             if mode == "mc2" and not noise_floor:
@@ -130,9 +132,11 @@ def main():
     ap.add_argument("--audit", type=float, default=0.01)
     ap.add_argument("--noise-floor", action="store_true")
     ap.add_argument("--xray-frontend", action="store_true", help="events from the GPU x-ray front end")
+    ap.add_argument("--lateral", type=float, default=50.0,
+                    help="depositions within this distance (um) of the detector centre go to the network")
     a = ap.parse_args()
     print(json.dumps(evaluate(a.model, a.config, a.xrays, a.seed, a.audit, noise_floor=a.noise_floor,
-                              frontend=a.xray_frontend)))
+                              frontend=a.xray_frontend, lateral_um=a.lateral)))
 
 
 if __name__ == "__main__":
