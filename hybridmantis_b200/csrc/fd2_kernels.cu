@@ -463,8 +463,15 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         // them wait (or nothing else runs)
         int fate = kAlive;
         if constexpr (kGrid) {
-            // explicit column lattice: one segment per round per live lane
-            if (alive) fate = w.grid_segment(a.g0);
+            // explicit column lattice: one segment per round per live lane;
+            // a lane in the gap waits until `fresnel_batch` lanes of the warp
+            // are in the gap (or no lane is in a column), so the gap's
+            // cell-by-cell search runs with more lanes at once.  Waiting only
+            // delays a photon's segments: its history is unchanged.
+            const unsigned gap = __ballot_sync(kFull, alive && w.in_gap);
+            const unsigned col = __ballot_sync(kFull, alive && !w.in_gap);
+            const bool go = alive && (!w.in_gap || (unsigned)__popc(gap) >= fresnel_min || col == 0);
+            if (go) fate = w.grid_segment(a.g0);
             if (alive && fate == kAlive) w.top_up();
         } else {
             if (alive && !parked && !xretry) {

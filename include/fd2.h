@@ -124,7 +124,9 @@ typedef struct fd2_options {
                                       shard of a larger stream draws the same
                                       random numbers as in the unsharded run     */
     int32_t fresnel_batch;         /* lanes parked at a column wall before the warp
-                                      runs their Fresnel interaction; 0 = tuned   */
+                                      runs their Fresnel interaction (with a
+                                      column lattice: lanes in the gap before the
+                                      warp runs their gap segments); 0 = tuned    */
     int32_t radial_bins;           /* > 0: label mode -- each history's detected
                                       photons are binned by distance r from their
                                       event instead of the PRF image: bin j <
