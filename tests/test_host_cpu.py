@@ -250,3 +250,19 @@ def test_ingest_entry_points_reject_null_handles():
     assert lib.fd2_ingest_push_um(None, None, None, None, None, None, 0) == 1
     assert lib.fd2_ingest_file(None, b"x") == 1
     assert lib.fd2_ingest_end(None, None) == 1
+
+
+def test_fd2run_usage():
+    """The command-line driver refuses incomplete or conflicting arguments before touching a GPU."""
+    import subprocess
+    exe = os.path.join(ROOT, "hybridmantis_b200", "bin", "fd2run")
+    inp = os.path.join(GOLDEN, "example_hybridMANTIS_input.in")
+    for args in ([], [inp], ["--xray", "pe.in", inp], ["--material", "m.mat", inp],
+                 ["--xray", "pe.in", "--material", "m.mat", inp, "events.txt"]):
+        r = subprocess.run([exe] + args, capture_output=True, text=True, timeout=60)
+        assert r.returncode == 2, (args, r.stderr)
+        assert "usage" in r.stderr
+    # a source section that cannot be read is reported, not run
+    r = subprocess.run([exe, "--xray", os.path.join(GOLDEN, "example_detected.txt"), "--material", "m.mat", inp],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "BIGS" in r.stderr
