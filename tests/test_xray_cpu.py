@@ -9,6 +9,8 @@ reference tree; what the reference does hold is the material file
   parser into tests/golden/csi_mat_raw.npz: cross sections at the file's
   nodes, the absorption edges, the electron CSDA range as the integral of
   1 / S, the transport mean free paths, the relaxation transitions;
+- the library's PENELOPE reader, run on a file in that format holding the
+  fixture's numbers, gives the committed tables;
 - the oracle's Rayleigh screening reproduces the file's Rayleigh cross
   section through its angular integral;
 - the oracle against closed forms: energy is conserved history by history;
@@ -275,3 +277,50 @@ def test_oracle_without_fluorescence():
     h, edes = run(xray.monoenergetic(50e3), 3000, seed=4, fluo=False)
     assert h["n_fe"].sum() == 0 and h["n_aug"].sum() == 0
     assert np.abs(balance(h, edes)).max() < 1e-6
+
+
+def write_penelope_file(path):
+    """A PENELOPE-format material file holding the fixture's numbers (energies up to 1 MeV)."""
+    L = [" PENELOPE (v. 2006)  Material data file ...............",
+         " Material: CESIUM IODIDE  (141)",
+         f" Mass density = {float(RAW['density']):.8E} g/cm**3",
+         f" Number of elements in the molecule =  {len(RAW['z'])}"]
+    for z, a in zip(RAW["z"], RAW["atoms"]):
+        L.append(f"   atomic number = {int(z)},  atoms/molecule = {a:.8E}")
+    for z in RAW["z"]:
+        sh, tr = RAW[f"relax_shells_{z}"], RAW[f"relax_trans_{z}"]
+        L.append(f" *** RELAX:  Z = {int(z)},  NO. OF SHELLS = {len(sh)},  NO. OF TRANSITIONS = {len(tr)}")
+        L += [f"  {int(d):2d} X 2  {e:.8E}" for d, e in sh]
+        L += [f"  {int(t[0]):2d} {int(t[1]):2d} {int(t[2]):2d}  {t[3]:.6E}  {t[4]:.6E}" for t in tr]
+    L.append(f" *** Stopping powers for electrons and positrons,  NDATA = {len(RAW['sp_e'])}")
+    L += [f" {e:.3E} {c:.5E} {r:.5E} {c:.5E} {r:.5E}" for e, c, r in zip(RAW["sp_e"], RAW["sp_col"], RAW["sp_rad"])]
+    L.append(f" ***  Electron and positron elastic cross sections,  NDATA = {len(RAW['el_e'])}")
+    L += [f" {e:.3E} {30 * s:.5E} {s:.5E} {2 * s:.5E} {30 * s:.5E} {s:.5E} {2 * s:.5E}"
+          for e, s in zip(RAW["el_e"], RAW["el_s1"])]
+    L.append(f" *** Rayleigh, Compton and pair-production cross sections,  NDATA = {len(RAW['rc_e'])}")
+    L += [f" {e:.3E} {r:.5E} {c:.5E} 0.00000E+00" for e, r, c in zip(RAW["rc_e"], RAW["rc_r"], RAW["rc_c"])]
+    for z in RAW["z"]:
+        a = RAW[f"pe_{z}"]
+        L.append(f" ***  Photoelectric cross sections,  IZ = {int(z)},  NSHELL =  {a.shape[1] - 2},  NDATA = {len(a)}")
+        L += [" " + " ".join(f"{v:.5E}" for v in row) for row in a]
+    L.append(" PENELOPE (v. 2006)  End of material data file ........")
+    path.write_text("\n".join(L) + "\n")
+
+
+def test_penelope_reader_on_a_material_file(tmp_path, mat):
+    """The library's PENELOPE reader on a file in that format (the fixture's numbers, to 1 MeV): the
+    same tables as the committed ones, which were read from the reference's own file."""
+    f = tmp_path / "CsI_1MeV.mat"
+    write_penelope_file(f)
+    m2 = xray.Material(str(f))
+    i1, i2 = mat.info(), m2.info()
+    for k in ("density", "molar_mass", "molecules_per_cm3", "z", "atoms", "k_edge_ev", "transitions"):
+        assert i1[k] == i2[k], k
+    E = np.geomspace(1.2e3, 9e5, 400)
+    np.testing.assert_allclose(m2.attenuation(E), mat.attenuation(E), rtol=1e-5)
+    r1, l1 = mat.electron(E)
+    r2, l2 = m2.electron(E)
+    np.testing.assert_allclose(r2, r1, rtol=1e-5)
+    np.testing.assert_allclose(l2, l1, rtol=1e-5)
+    # the Rayleigh screening solved from the parsed cross sections: same samples as the oracle's
+    assert i2["rayleigh_screening_cm"] == pytest.approx(i1["rayleigh_screening_cm"], rel=1e-5)
