@@ -11,8 +11,14 @@ photon counts ~ Poisson(E * 54/keV) sampled on the GPU each step.
   e2e     photons/s through the C ABI with host buffers: H2D of the EDE
           buffer (cm / eV / history), transport, D2H of PRF + PHS + stats
   roofline  the transport kernel against the FP32 issue roofline
-  cpu_baseline  the reference's own C transport (oracle/_ref, gcc -O2,
-          all host cores) on a bounded sample of the same stream
+  cpu_baseline  the reference's own C transport (oracle/_ref) on a bounded
+          sample of the same stream and photon counts: all host cores at
+          gcc -O2 (the value), one core at -O2 and one core at -O0 (the
+          reference's own flags), with the CPU model
+  results.parity  the GPU's FP32 tallies on the cpu_baseline sample's
+          events and photon counts against the reference C's: fate z-scores,
+          PHS mean and Swank z-scores and relative errors, per-bin PRF
+          chi-square
   reference_gpu the reference's own CUDA kernel `algo` (oracle/_ref,
           compiled for sm_100a with its own flags) on the same events and
           photon counts, one launch of its 18000 x 128 grid
@@ -103,11 +109,13 @@ def _cpu_cores() -> int:
 def _ref_worker(args):
     sys.path.insert(0, ROOT)
     from oracle import pyoracle as po
-    geom, x, y, z, hist, nphot, base, prim_size = args
+    geom, x, y, z, hist, nphot, base, prim_size, opt, keep = args
     t0 = time.perf_counter()
     r = po.run_ref(geom, x, y, z, hist, nphot, seed_input=271828182, base=base, prim_size=prim_size,
-                   records=False, opt="O2")
-    return time.perf_counter() - t0, int(r.counters[0])
+                   records=False, opt=opt)
+    dt = time.perf_counter() - t0
+    tallies = (r.image, r.per_primary, r.counters) if keep else None
+    return dt, int(r.counters[0]), tallies
 
 
 def _oracle_geometry(p):
@@ -117,8 +125,20 @@ def _oracle_geometry(p):
                        lb_x=p.lb_x, lb_y=p.lb_y, ub_x=p.ub_x, ub_y=p.ub_y, sensor_refl=p.sensor_refl, pixel=p.pixel)
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 class CpuReference:
-    """The reference's C transport (oracle/_ref, -O2) on all host cores; one
+    """The reference's C transport (oracle/_ref) on the host cores; one
     process per core over contiguous event slices (each event keeps its own
     RANECU stream, so the split does not change results)."""
 
@@ -131,31 +151,128 @@ class CpuReference:
         self.pool = ProcessPoolExecutor(self.cores, mp_context=mp.get_context("spawn"))
         # pilot on one core to size samples
         k = self._events_for(20000, 0)
-        dt, ph = _ref_worker(self._args(0, k))
+        dt, ph, _ = self.pool.submit(_ref_worker, self._args(0, k, "O2", False)).result()
         self.rate1 = ph / max(dt, 1e-6)
 
     def _events_for(self, photons, start):
         c = np.cumsum(self.N[start:])
         return int(min(len(c), np.searchsorted(c, photons) + 1))
 
-    def _args(self, start, count):
+    def _args(self, start, count, opt, keep):
         es = self.es
         sl = slice(start, start + count)
         return (self.g, es.x_um[sl].astype(np.float64), es.y_um[sl].astype(np.float64),
-                es.z_um[sl].astype(np.float64), es.hist[sl], self.N[sl], start, int(es.params.num_hist))
+                es.z_um[sl].astype(np.float64), es.hist[sl], self.N[sl], start, int(es.params.num_hist), opt, keep)
 
-    def timed_sample(self, seconds, start=0):
-        photons = self.rate1 * self.cores * seconds
+    def timed_sample(self, seconds, start=0, cores=None, opt="O2", keep=False, rate=None):
+        """Transport about `seconds` of work from event `start` on `cores`
+        processes; returns photons/s, photons, events, seconds and (keep) the
+        summed tallies (image, per-primary counts, counters)."""
+        cores = cores or self.cores
+        photons = (rate or self.rate1) * cores * seconds
         count = self._events_for(photons, start)
-        bounds = np.linspace(start, start + count, self.cores + 1).astype(int)
+        bounds = np.linspace(start, start + count, cores + 1).astype(int)
         t0 = time.perf_counter()
-        futs = [self.pool.submit(_ref_worker, self._args(a, b - a)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
-        ph = sum(f.result()[1] for f in futs)
+        futs = [self.pool.submit(_ref_worker, self._args(a, b - a, opt, keep))
+                for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+        res = [f.result() for f in futs]
         dt = time.perf_counter() - t0
-        return ph / dt, ph, count, dt
+        ph = sum(r[1] for r in res)
+        tallies = None
+        if keep:
+            img = sum(r[2][0] for r in res)
+            prim = sum(r[2][1] for r in res)
+            cnt = sum(r[2][2] for r in res)
+            tallies = (img, prim, cnt)
+        return ph / dt, ph, count, dt, tallies
 
     def close(self):
         self.pool.shutdown()
+
+
+def cpu_variants(ref, seconds_one_core=6.0):
+    """One core at -O2 and at -O0 (the reference's own compile flags,
+    main/compile_ver1_0.sh:10) on the first events of the stream."""
+    out = {}
+    for opt in ("O2", "O0"):
+        rate = ref.rate1 if opt == "O2" else ref.rate1 / 2.5
+        r, ph, nev, dt, _ = ref.timed_sample(seconds_one_core, cores=1, opt=opt, rate=rate)
+        out[f"1core_{opt}"] = {"value": r, "unit": "photons/s", "cores": 1, "flags": f"gcc -{opt}",
+                               "sample": f"first {nev} events ({ph} photons), {dt:.1f} s"}
+    return out
+
+
+# ---------------------------------------------------------- parity stats
+
+def _phs_moments(per_primary):
+    c = np.asarray(per_primary, np.float64)
+    c = c[c > 0]
+    n = len(c)
+    m1, m2 = c.mean(), (c * c).mean()
+    g = np.array([2 * m1 / m2, -m1 * m1 / (m2 * m2)])
+    cov = np.cov(np.vstack([c, c * c]), ddof=1) / n
+    return {"n": n, "mean": m1, "se_mean": c.std(ddof=1) / np.sqrt(n), "swank": m1 * m1 / m2,
+            "se_swank": float(np.sqrt(g @ cov @ g))}
+
+
+def _z_binomial(k1, n1, k2, n2):
+    p = (k1 + k2) / (n1 + n2)
+    return (k1 / n1 - k2 / n2) / np.sqrt(max(p * (1 - p) * (1 / n1 + 1 / n2), 1e-300))
+
+
+def _chi2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    m = (a + b) > 0
+    return float((((a - b) ** 2) / (a + b))[m].sum()), int(m.sum())
+
+
+def parity_vs_reference(es, nphot, nev, ref_tallies, device, seed):
+    """The GPU's FP32 production transport against the reference C on the
+    same events (the first `nev` of the stream) and the same photon counts:
+    z-scores of the fate fractions, the PHS mean and the Swank factor, and a
+    per-bin Poisson chi-square of the PRF (central 41 x 41 one-micron pixels
+    around the beam plus ring totals outside them)."""
+    import hybridmantis_b200 as hb
+    img_r, prim_r, cnt_r = ref_tallies
+    N = np.asarray(nphot[:nev], np.int32)
+    sub = es.subset(slice(0, nev))
+    with hb.OpticalTransport(es.params, device=device, count_mode=hb.COUNT_GIVEN, seed=seed) as t:
+        t.submit(sub, nphot=N)
+        t.run_sync()
+        c = t.counters()
+        prim = t.detected_per_primary()
+        img = t.prf()
+    n = int(N.sum())
+    names = ["detected", "abs_top", "abs_bulk", "lost", "outofcol", "theta1"]
+    ref = dict(zip(names, [int(v) for v in cnt_r[1:7]]))
+    z_f = {k: float(_z_binomial(c[k], n, ref[k], n)) for k in names[:4]}
+    g, o = _phs_moments(prim), _phs_moments(prim_r)
+    z_mean = (g["mean"] - o["mean"]) / np.hypot(g["se_mean"], o["se_mean"])
+    z_swank = (g["swank"] - o["swank"]) / np.hypot(g["se_swank"], o["se_swank"])
+    p = es.params
+    cx = int(np.floor((np.median(sub.x_um) - p.lb_x) / p.pixel))
+    cy = int(np.floor((np.median(sub.y_um) - p.lb_y) / p.pixel))
+    a = np.asarray(img, np.float64)
+    b = np.asarray(img_r, np.float64)[:a.shape[0], :a.shape[1]]
+    box = (slice(cx - 20, cx + 21), slice(cy - 20, cy + 21))
+    chi_core, dof_core = _chi2(a[box].ravel(), b[box].ravel())
+    a[box] = 0.0
+    b[box] = 0.0
+    ii, jj = np.meshgrid(np.arange(a.shape[0]) + 0.5, np.arange(a.shape[1]) + 0.5, indexing="ij")
+    r = np.hypot(ii - (cx + 0.5), jj - (cy + 0.5)).ravel()
+    edges = np.array([20.5, 25, 30, 40, 55, 75, 100, 140, 200, 300, 400])
+    chi_ring, dof_ring = _chi2(np.histogram(r, edges, weights=a.ravel())[0], np.histogram(r, edges, weights=b.ravel())[0])
+    chi2, dof = chi_core + chi_ring, dof_core + dof_ring
+    return {"sample": f"first {nev} events of the step's stream, {n} photons, the step's photon counts",
+            "against": "reference C transport (oracle/_ref, main/kernel_cuda_c_ver1_0.cu C path)",
+            "z_fates": z_f, "z_phs_mean": float(z_mean), "z_swank": float(z_swank),
+            "phs_mean": {"gpu": g["mean"], "reference": o["mean"], "rel_err": g["mean"] / o["mean"] - 1.0,
+                         "se": float(np.hypot(g["se_mean"], o["se_mean"]))},
+            "swank": {"gpu": g["swank"], "reference": o["swank"], "rel_err": g["swank"] / o["swank"] - 1.0,
+                      "se": float(np.hypot(g["se_swank"], o["se_swank"]))},
+            "prf_chi2": chi2, "prf_dof": dof, "prf_chi2_per_dof": chi2 / max(dof, 1),
+            "prf_z": float((chi2 - dof) / np.sqrt(2.0 * max(dof, 1)))}
 
 
 # DRAM bytes per photon of the transport kernel: dram__bytes_read.sum +
@@ -163,9 +280,41 @@ class CpuReference:
 # of the config-1 stream, 2,000 x-rays); the traffic is one event record per
 # chunk and grows in proportion to the photons.
 TRANSPORT_DRAM_BYTES_PER_PHOTON = 3338240.0 / 4690971.0
-# Issue slots the transport kernel uses in steady state (ncu
-# smsp__issue_active of 20,000 config-1 x-rays, where its tail is small).
-TRANSPORT_ISSUE_ACTIVE = 0.554
+# ncu counters of the transport kernel in steady state (one capture of this
+# build on 20,000 config-1 x-rays, where the launch's tail is small): issue
+# slots used (smsp__issue_active), FP32 FMA pipe busy (sm__pipe_fma_cycles_
+# active), active lanes per warp instruction (smsp__thread_inst_executed_per_
+# inst_executed) and warp instructions per photon (smsp__inst_executed.sum /
+# photons).
+TRANSPORT_NCU = {"issue_slot_utilisation": 0.554, "fp32_pipe_utilisation": 0.232,
+                 "lanes_per_instruction": 16.43, "warp_instructions_per_photon": 1628.0,
+                 "source": "ncu --clock-control none on 20,000 config-1 x-rays (transport_kernel<false,320,2>)"}
+
+
+def bench_config(es, world):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "events_per_step": int(es.n), "xrays_per_step": int(es.params.num_hist),
+            "photon_counts": "N ~ Poisson(E x 54/keV) per event",
+            "l2": "GPU arm: 256 MiB buffer written between timed steps (inside the timed region)",
+            "parallelism": f"weak-scaling x{world}" if world > 1 else "single GPU"}
+
+
+def measure_fp32_peak(device, seconds=2.0):
+    """FP32 FMA throughput measured by the library's microbenchmark kernel,
+    with the SM clock sampled while it runs."""
+    import ctypes
+    import hybridmantis_b200 as hb
+    tf, dt = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    with ClockSampler(device) as clk:
+        st = hb.load().fd2_measure_fp32_peak(device, seconds, ctypes.byref(tf), ctypes.byref(dt))
+    if st != 0:
+        return None
+    c = clk.summary()
+    out = {"tflops": tf.value, "seconds": dt.value, "sm_mhz": c["sm_mhz"], "sm_max_mhz": c["sm_max_mhz"],
+           "reasons": c["reasons"]}
+    if c["sm_mhz"] and c["sm_max_mhz"]:
+        out["tflops_at_max_clock"] = tf.value * c["sm_max_mhz"] / c["sm_mhz"]
+    return out
 
 
 def reference_gpu(es, nphot, device):
@@ -321,7 +470,7 @@ def run_ours(a, rank, world, local_rank):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    es = hb.synth_events(a.config, a.xrays, a.seed + 7919 * rank)
+    es = hb.synth_events(a.config, a.xrays, a.seed + 7919 * rank)  # rank 0: the reference arm's stream
     x, y, z = es.to_cm()
     de = es.e_ev.astype(np.float64)
     t = hb.OpticalTransport(es.params, device=local_rank, seed=0x5eed + rank,
@@ -419,6 +568,7 @@ def run_ours(a, rank, world, local_rank):
         photons_per_launch = tm["photons"]
         avg_kern_s = float(np.mean(kern_ms)) / 1e3
         achieved = photons_per_launch * wpp / avg_kern_s / 1e12
+        fma = measure_fp32_peak(local_rank) if world == 1 else None
         roofline = {"bound": "fp32-issue", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                     "frac": achieved / peak_tflops,
                     "traffic": TRANSPORT_DRAM_BYTES_PER_PHOTON * photons_per_launch,
@@ -426,21 +576,25 @@ def run_ours(a, rank, world, local_rank):
                                       "scaled by photons",
                     "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 (FMA) x {sm_max:.0f} MHz "
                                    f"(sm_max_mhz of MEASURED_PEAKS.json; the file has no FP32 entry)",
+                    "peak_measured_fma": fma,
                     "work_per_photon_fp32_ops": wpp, "kernel_ms_per_launch": avg_kern_s * 1e3,
                     "photons_per_launch": photons_per_launch,
-                    # the north-star criterion for this issue-bound kernel: scheduler issue slots used
-                    "issue_slot_utilisation": TRANSPORT_ISSUE_ACTIVE,
-                    "issue_slot_source": "ncu smsp__issue_active.avg.pct_of_peak_sustained_active of the same "
-                                         "kernel on 20,000 config-1 x-rays (steady state, "
-                                         "profiles/transport_kernel_config1_20k.md)"}
+                    "ncu": TRANSPORT_NCU}
         cpu = None
+        parity = None
         if not a.no_cpu_baseline and world == 1:
             ref = CpuReference(es, nphot)
-            rate, ph, nev, dt = ref.timed_sample(a.cpu_seconds)
+            rate, ph, nev, dt, tallies = ref.timed_sample(a.cpu_seconds, keep=True)
+            variants = cpu_variants(ref)
             ref.close()
             cpu = {"value": rate, "unit": "photons/s", "cores": ref.cores, "kind": "reference",
+                   "cpu_model": cpu_model(),
                    "sample": f"first {nev} events ({ph} photons) of the same stream and the same photon counts, "
-                             f"reference C transport (gcc -O2), {ref.cores} processes, {dt:.1f} s"}
+                             f"reference C transport (gcc -O2), {ref.cores} processes, {dt:.1f} s",
+                   "variants": dict(variants, **{f"{ref.cores}core_O2": {
+                       "value": rate, "unit": "photons/s", "cores": ref.cores, "flags": "gcc -O2",
+                       "sample": f"first {nev} events ({ph} photons), {dt:.1f} s"}})}
+            parity = parity_vs_reference(es, nphot, nev, tallies, local_rank, seed=0xa11ce)
         ref_gpu = None
         if not a.no_ref_gpu and world == 1:
             ref_gpu = reference_gpu(es, nphot, local_rank)
@@ -468,12 +622,8 @@ def run_ours(a, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded EDE generator; PENELOPE not shipped)",
-            "config": {"workload": WORKLOAD, "events_per_step": es.n, "xrays_per_step": es.params.num_hist,
-                       "photons_per_step": photons / max(a.steps, 1) / world,
-                       "l2": "256 MiB buffer written between timed steps (inside the timed region)",
-                       "parallelism": f"weak-scaling x{world}" if world > 1 else "single GPU",
-                       "launch": {k: tm[k] for k in ("grid", "block", "chunk", "refill", "prf_window",
-                                                           "fresnel_batch")}},
+            "config": bench_config(es, world),
+            "launch": {k: tm[k] for k in ("grid", "block", "chunk", "refill", "prf_window", "fresnel_batch")},
             "e2e": {"value": e2e_photons / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             # per step: count, scan_tiles, scan_sums, scan_add, fill_chunks, transport, phs, bump
@@ -489,7 +639,8 @@ def run_ours(a, rank, world, local_rank):
                                              ("detected", "abs_top", "abs_bulk", "lost", "outofcol", "theta1",
                                               "capped")},
                         "xrays_per_s": es.params.num_hist * a.steps * world / (ms / 1e3),
-                        "merge_ms": merge_ms, "calls_per_photon": calls},
+                        "photons_per_step": photons / max(a.steps, 1) / world,
+                        "merge_ms": merge_ms, "calls_per_photon": calls, "parity": parity},
         }
     t.close()
     if dist:
@@ -499,23 +650,26 @@ def run_ours(a, rank, world, local_rank):
 
 # --------------------------------------------------------- reference arm
 
-def run_reference(a, rank):
+def run_reference(a, rank, world):
+    """The reference's own C transport (oracle/_ref, gcc -O2) on every host
+    core, over the same event stream as the product arm (the generator's
+    host-only build in oracle/, so this process maps no product library) with
+    photon counts N ~ Poisson(E * yield) drawn on the host, as the reference's
+    driver does with GSL (numpy stands in for GSL)."""
     if rank != 0:
         return None
-    import hybridmantis_b200 as hb
-    es = hb.synth_events(a.config, a.xrays, a.seed)
+    from oracle import pyoracle as po
+    es = po.synth_events_host(a.config, a.xrays, a.seed)
     rng = np.random.default_rng(a.seed)
-    # the reference samples N ~ Poisson(E * yield) on the host (GSL); numpy here
     nphot = rng.poisson(es.e_ev.astype(np.float64) * es.params.yield_).astype(np.int32)
     ref = CpuReference(es, nphot)
     per_step_s = max(1.0, min(6.0, 150.0 / max(a.steps + a.warmup, 1)))
     start = 0
     for _ in range(a.warmup):
         ref.timed_sample(per_step_s / 2, start)
-    rates, total_ph, total_t, nev_tot = [], 0, 0.0, 0
+    total_ph, total_t, nev_tot = 0, 0.0, 0
     for _ in range(a.steps):
-        rate, ph, nev, dt = ref.timed_sample(per_step_s, start)
-        rates.append(rate)
+        rate, ph, nev, dt, _ = ref.timed_sample(per_step_s, start)
         total_ph += ph
         total_t += dt
         nev_tot += nev
@@ -525,13 +679,14 @@ def run_reference(a, rank):
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_t / a.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (double libm intermediates)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded EDE generator; PENELOPE not shipped)",
-        "config": {"workload": WORKLOAD, "events_per_step": es.n, "sample_per_step_s": per_step_s},
+        "config": bench_config(es, world),
         "cpu_baseline": {"value": value, "unit": "photons/s", "cores": ref.cores, "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": f"{a.steps} samples of ~{per_step_s:.1f} s ({nev_tot} events, {total_ph} photons) "
-                                   f"of the config-1 stream, reference C transport compiled in place (gcc -O2), "
-                                   f"one process per core"},
+                                   f"of the config-1 stream, reference C transport compiled in place (gcc -O2, "
+                                   f"float walk with double libm intermediates), one process per core"},
         "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -542,7 +697,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
-        out = run_reference(a, rank)
+        out = run_reference(a, rank, world)
     else:
         out = run_ours(a, rank, world, local_rank)
     if rank == 0 and out is not None:

@@ -176,7 +176,7 @@ EXPORTED = [
     "fd2_reset_tallies", "fd2_get_counters", "fd2_get_prf_dims", "fd2_get_prf",
     "fd2_get_detected_per_primary", "fd2_get_radial", "fd2_get_photon_counts", "fd2_get_phs", "fd2_get_phs_stats",
     "fd2_get_timing", "fd2_get_stream", "fd2_write_outputs", "fd2_write_output_files", "fd2_replay",
-    "fd2_autotune", "fd2_transport_noalloc",
+    "fd2_autotune", "fd2_transport_noalloc", "fd2_measure_fp32_peak", "fd2_debug_wall_root",
     "fd2_synth_events", "fd2_free_events", "fd2_read_events_text", "fd2_write_events_text",
     "fd2_read_events_binary", "fd2_write_events_binary",
     "fd2_ingest_begin", "fd2_ingest_push", "fd2_ingest_push_um", "fd2_ingest_file", "fd2_ingest_end",
@@ -214,6 +214,9 @@ def load():
         "fd2_params_to_geometry": (ctypes.c_int, [P(Params), P(Geometry)]),
         "fd2_prf_dims": (ctypes.c_int, [P(Geometry), P(ctypes.c_int32), P(ctypes.c_int32)]),
         "fd2_create": (ctypes.c_int, [P(Params), P(Options), P(vp)]),
+        "fd2_debug_wall_root": (ctypes.c_int, [ctypes.c_int32, vp, vp, vp, vp]),
+        "fd2_measure_fp32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_double, P(ctypes.c_double),
+                                                 P(ctypes.c_double)]),
         "fd2_destroy": (None, [vp]),
         "fd2_last_error": (ctypes.c_char_p, [vp]),
         "fd2_set_geometries": (ctypes.c_int, [vp, P(Geometry), ctypes.c_int32]),

@@ -613,6 +613,15 @@ __global__ void phs_kernel(int32_t n_prim, const int32_t *__restrict__ per_prima
 
 __global__ void bump_kernel(uint32_t *run_tag) { *run_tag += 1u; }
 
+// The walk's wall root (the far intersection with the column) for given
+// quadratic coefficients, compiled with the transport's flags.
+__global__ void wall_root_kernel(int n, const float *__restrict__ qa, const float *__restrict__ qb,
+                                 const float *__restrict__ qc, float *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = wall_root(qa[i], qb[i], qc[i]);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- launchers
@@ -774,3 +783,29 @@ cudaError_t launch_phs(cudaStream_t s, int32_t n_prim, const int32_t *per_primar
 }
 
 }  // namespace fd2
+
+// Diagnostic entry point (tests): evaluates the transport's wall-root routine
+// on the current device for n quadratics a t^2 + b t + c = 0 given in host
+// arrays, so a test can drive its FP64 fallback for a nearly cancelling
+// discriminant.  Synchronous.
+extern "C" __attribute__((visibility("default"))) int fd2_debug_wall_root(int32_t n, const float *qa, const float *qb,
+                                                                          const float *qc, float *out)
+{
+    if (n < 0 || (n > 0 && (!qa || !qb || !qc || !out))) return 1;
+    if (n == 0) return 0;
+    float *d = nullptr;
+    const size_t b = sizeof(float) * (size_t)n;
+    cudaError_t e = cudaMalloc(&d, 4 * b);
+    if (e != cudaSuccess) return 5;
+    if (e == cudaSuccess) e = cudaMemcpy(d, qa, b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + n, qb, b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + 2 * (size_t)n, qc, b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        fd2::wall_root_kernel<<<(unsigned)((n + 255) / 256), 256>>>(n, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 3 * (size_t)n, b, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : 4;
+}
+

@@ -34,6 +34,7 @@ namespace {
 constexpr int64_t kNaMaxEvents = 262144;
 constexpr int64_t kNaMaxChunks = 2097152;
 constexpr int kNaChunk = 256;  // photons per queue chunk
+constexpr int64_t kNaMaxPerEvent = 900000;  // photons per event (the reference's own cap)
 constexpr int kNaMaxDevices = 64;
 
 // Scratch layout (bytes, each part 256-byte aligned).
@@ -66,6 +67,17 @@ __global__ void noalloc_pack(int64_t n, const float *__restrict__ x, const float
             atomicOr(status, fd2::kStatusBadEvent);
         pos[i] = make_float4(x[i], y[i], z[i], __int_as_float(h - 1));
     }
+}
+
+// Runs between the queue construction and the transport: when the call is
+// going to be rejected (a flagged event, an event above the photon cap, more
+// chunks than the scratch holds -- fill_chunks then leaves stale descriptors
+// of an earlier call behind the ones it wrote), the queue is emptied so the
+// transport tallies nothing and the caller's buffers stay as they were.
+__global__ void noalloc_guard(const int *status, unsigned long long *n_chunks)
+{
+    constexpr int kReject = fd2::kStatusBadEvent | fd2::kStatusTooManyPhotons | fd2::kStatusChunkOverflow;
+    if (threadIdx.x == 0 && (*status & kReject)) *n_chunks = 0ull;
 }
 
 fd2_status scratch_for_current_device(unsigned char **out)
@@ -167,11 +179,15 @@ extern "C" fd2_status fd2_transport_noalloc(const fd2_geometry *geometry, const 
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)
-        e = fd2::launch_count(s, n, 0, fd2::kCountGiven, 0.0, 900000, seed, reinterpret_cast<const uint32_t *>(flags + 1),
+        e = fd2::launch_count(s, n, 0, fd2::kCountGiven, 0.0, kNaMaxPerEvent, seed, reinterpret_cast<const uint32_t *>(flags + 1),
                               cfg.chunk, nullptr, nphot, nullptr, pos, ev_n, nchunks, scalars + 3, nullptr, nullptr,
                               num_hist, flags);
     if (e == cudaSuccess) e = fd2::launch_scan(s, n, nchunks, offsets, block_sums, scalars + 0);
     if (e == cudaSuccess) e = fd2::launch_fill_chunks(s, n, cfg.chunk, ev_n, offsets, chunks, kNaMaxChunks, flags);
+    if (e == cudaSuccess) {
+        noalloc_guard<<<1, 32, 0, s>>>(flags, scalars + 0);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = fd2::prepare_transport(cfg, 1);
     if (e == cudaSuccess) {
         fd2::TransportArgs a;

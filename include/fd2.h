@@ -264,8 +264,14 @@ FD2_API fd2_status fd2_replay(fd2_ctx *ctx, int32_t mode, int32_t seed_input,
  * into prf (xdim*ydim u64, [ii*ydim + jj]), per_primary (num_hist int32,
  * index hist-1) and counters (9 u64: unused, detected, abs_top, abs_bulk,
  * lost, outofcol, theta1, capped, detected in the PRF).  At most 262144
- * events and 2097152 work-queue chunks of 256 photons per call; larger
- * inputs return FD2_ERR_INVALID_ARGUMENT.  The work queue lives in one
+ * events, 900000 photons per event and 2097152 work-queue chunks of 256
+ * photons per call.  More events return FD2_ERR_INVALID_ARGUMENT at once;
+ * more chunks return FD2_ERR_INVALID_ARGUMENT, an event above 900000
+ * photons FD2_ERR_TOO_MANY_PHOTONS and an invalid event (non-finite
+ * position, history outside 1..num_hist, negative count) FD2_ERR_BAD_EVENT
+ * after the device has checked them; a call that fails in any of these
+ * ways transports nothing and leaves prf, per_primary and counters as they
+ * were.  The work queue lives in one
  * fixed ~24 MiB __device__ array that every GPU loading the library holds
  * until exit; the first call on a device looks up its address (make it
  * before any stream capture on that device).  Calls share that array:
@@ -277,6 +283,21 @@ FD2_API fd2_status fd2_transport_noalloc(const fd2_geometry *geometry, const flo
                                          const float *z_um, const int32_t *hist, const int32_t *nphot, int64_t n,
                                          int32_t num_hist, uint64_t seed, uint64_t *prf, int32_t *per_primary,
                                          uint64_t *counters, void *stream);
+
+/* FP32 fused multiply-add throughput of `device`, the transport's roofline
+ * denominator measured instead of derived: a kernel of independent FMA
+ * chains over every SM, launched repeatedly for at least `min_seconds`
+ * (CUDA events); *tflops is the best launch (2 flops per FMA), *seconds the
+ * time spent (may be NULL).  No counterpart in the reference. */
+FD2_API fd2_status fd2_measure_fp32_peak(int32_t device, double min_seconds, double *tflops, double *seconds);
+
+/* Diagnostic (tests): the transport's column-wall root routine on the
+ * current device for n quadratics a t^2 + b t + c = 0 (host arrays in and
+ * out; the larger root, 999 where there is none).  Its FP64 fallback for a
+ * nearly cancelling discriminant is the compensated quadratic of the walk
+ * (dist_to_surface, main/kernel_cuda_c_ver1_0.cu:966-1186, has none).
+ * Returns an fd2_status value. */
+FD2_API int fd2_debug_wall_root(int32_t n, const float *qa, const float *qb, const float *qc, float *out);
 
 /* Autotuner: times transport configurations on the resident events and
  * keeps the fastest (cached in options.tune_cache when set). */

@@ -37,8 +37,11 @@
 enum { C_GEN, C_DETECT, C_ABS_TOP, C_ABS_BULK, C_LOST, C_OUTOFCOL, C_THETA1 };
 
 /* Call counts of the transport's building blocks (reset by
- * fd2o_reset_call_counts); used to express the work per photon. */
-static uint64_t o_calls[FD2O_NCALLS];
+ * fd2o_reset_call_counts); used to express the work per photon.  One set
+ * per host thread: callers that run event slices on several threads do not
+ * share (or fight over) the counters, and a reset / read sees the calling
+ * thread's calls only. */
+static _Thread_local uint64_t o_calls[FD2O_NCALLS];
 #define O_CALL(k) (o_calls[(k)]++)
 
 void fd2o_reset_call_counts(void) { memset(o_calls, 0, sizeof o_calls); }

@@ -89,7 +89,8 @@ int fd2o_run(const fd2o_geom *g, int n_events,
              int8_t *fate, int32_t *pix, int32_t *seeds, int32_t *steps);
 
 /* Call counts of the transport's building blocks since the last reset,
- * FD2O_NCALLS entries indexed by FD2O_CALL_*. */
+ * FD2O_NCALLS entries indexed by FD2O_CALL_*; counted per host thread (a
+ * reset and a read see the calling thread's transport calls). */
 enum {
     FD2O_CALL_STEP, FD2O_CALL_TO_WALL, FD2O_CALL_PULLBACK, FD2O_CALL_SURFACE, FD2O_CALL_INCIDENCE,
     FD2O_CALL_FRESNEL, FD2O_CALL_REFLECT, FD2O_CALL_REFRACT, FD2O_CALL_CROSSTALK, FD2O_CALL_HOP,

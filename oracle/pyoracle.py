@@ -23,6 +23,7 @@ ORACLE_SO = os.path.join(HERE, "_build", "libfd2oracle.so")
 REF_SO = {"O0": os.path.join(HERE, "_ref", "libfd2ref_O0.so"),
           "O2": os.path.join(HERE, "_ref", "libfd2ref_O2.so")}
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libfd2refcuda.so")
+SYNTH_SO = os.path.join(HERE, "_build", "libfd2synth.so")
 
 FATE_NAMES = {0: "none", 1: "detect", 2: "abs_top", 3: "abs_bulk", 4: "lost",
               5: "outofcol", 6: "theta1"}
@@ -260,3 +261,47 @@ def run_ref_cuda(g: Geometry, x, y, z, hist, nphot, num_hist: int, grid: int = 1
     if rc != 0:
         raise RuntimeError(f"fd2refcu_run returned {rc} (CUDA error {err.value})")
     return RunResult(image.reshape(xdim, ydim), prim, cnt, extra={"kernel_ms": float(ms.value)})
+
+
+@dataclass
+class HostEvents:
+    """A synthetic EDE stream built on the host (micrometres, eV, 1-based
+    histories) with the benchmark configuration's parameters."""
+    x_um: np.ndarray
+    y_um: np.ndarray
+    z_um: np.ndarray
+    e_ev: np.ndarray
+    hist: np.ndarray
+    params: object
+    num_hist: int
+
+    @property
+    def n(self) -> int:
+        return len(self.x_um)
+
+
+def synth_events_host(config: int, num_xrays: int = 0, seed: int = 12345) -> HostEvents:
+    """The seeded synthetic EDE stream of benchmark configuration ``config``
+    from the host-only build of the product's generator (_build/libfd2synth.so):
+    the same events as ``hybridmantis_b200.synth_events`` with the same
+    arguments, without loading the product library (bench.py's reference arm
+    runs in a process that maps no product code)."""
+    from hybridmantis_b200._lib import Events  # ctypes layouts only; loads no library
+
+    lib = _load(SYNTH_SO)
+    ev = Events()
+    lib.fd2_synth_events.restype = ctypes.c_int
+    rc = lib.fd2_synth_events(ctypes.c_int32(config), ctypes.c_int32(num_xrays), ctypes.c_uint64(seed),
+                              ctypes.byref(ev))
+    if rc != 0:
+        raise ValueError(f"fd2_synth_events returned {rc}")
+    n = int(ev.n)
+
+    def arr(p, dt):
+        return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n and p else np.zeros(0, dt)
+
+    out = HostEvents(arr(ev.x_um, np.float32), arr(ev.y_um, np.float32), arr(ev.z_um, np.float32),
+                     arr(ev.e_ev, np.float32), arr(ev.hist, np.int32), type(ev.params).from_buffer_copy(ev.params),
+                     int(ev.num_hist))
+    lib.fd2_free_events(ctypes.byref(ev))
+    return out

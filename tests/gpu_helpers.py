@@ -65,3 +65,55 @@ def report(name, payload):
     os.makedirs(d, exist_ok=True)
     with open(os.path.join(d, f"{name}.json"), "w") as f:
         json.dump(payload, f, indent=1, default=lambda o: o.tolist() if hasattr(o, "tolist") else str(o))
+
+
+def run_oracle_parallel(es, N, params=None, seed_input=271828182, workers=None):
+    """The oracle over contiguous event slices on host threads (ctypes
+    releases the GIL during the call).  Event e keeps its own RANECU stream
+    init_PRNG(base + e), so the summed tallies equal one call over all events
+    (tests/test_oracle_cpu.py checks this)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    p = params or es.params
+    g = oracle_geometry(p)
+    n = es.n
+    workers = workers or max(1, min(len(os.sched_getaffinity(0)), 32))
+    N = np.asarray(N, np.int32)
+    # equal photon shares per slice
+    cum = np.concatenate([[0], np.cumsum(N, dtype=np.int64)])
+    cuts = np.searchsorted(cum, np.linspace(0, cum[-1], workers + 1)).clip(0, n)
+    cuts[0], cuts[-1] = 0, n
+    cuts = np.unique(cuts)
+
+    def one(a, b):
+        return po.run_oracle(g, es.x_um[a:b].astype(np.float64), es.y_um[a:b].astype(np.float64),
+                             es.z_um[a:b].astype(np.float64), es.hist[a:b], N[a:b], seed_input=seed_input, base=int(a),
+                             prim_size=p.num_hist, records=False)
+
+    with ThreadPoolExecutor(len(cuts) - 1) as ex:
+        parts = list(ex.map(lambda ab: one(*ab), zip(cuts[:-1], cuts[1:])))
+    out = parts[0]
+    for r in parts[1:]:
+        out.image += r.image
+        out.per_primary += r.per_primary
+        out.counters += r.counters
+    return out
+
+
+def given_counts(es, seed):
+    """Poisson(E * yield) photon counts fixed on the host."""
+    rng = np.random.default_rng(seed)
+    return rng.poisson(es.e_ev.astype(np.float64) * es.params.yield_).astype(np.int32)
+
+
+def geometry_params(es, g):
+    """Params of geometry g of a batched stream (the base params with the
+    geometry's fields)."""
+    p = hb.default_params()
+    for f, _ in p._fields_:
+        setattr(p, f, getattr(es.params, f))
+    geo = es.geometries[g]
+    for f, _ in geo._fields_:
+        if f != "reserved" and hasattr(p, f):
+            setattr(p, f, getattr(geo, f))
+    return p

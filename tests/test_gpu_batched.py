@@ -15,29 +15,12 @@ import pytest
 import hybridmantis_b200 as hb
 from oracle import pyoracle as po
 
-from gpu_helpers import oracle_geometry, report
+from gpu_helpers import geometry_params, given_counts, oracle_geometry, report
 from mcstats import phs_moments, z_binomial
 
 pytestmark = pytest.mark.gpu
 FATES = ["detected", "abs_top", "abs_bulk", "lost"]
 ORACLE_FATES = {"detected": 1, "abs_top": 2, "abs_bulk": 3, "lost": 4}
-
-
-def given_counts(es, seed):
-    rng = np.random.default_rng(seed)
-    return rng.poisson(es.e_ev.astype(np.float64) * es.params.yield_).astype(np.int32)
-
-
-def geometry_params(es, g):
-    """Params of geometry g (the base params with the geometry's fields)."""
-    p = hb.default_params()
-    for f, _ in p._fields_:
-        setattr(p, f, getattr(es.params, f))
-    geo = es.geometries[g]
-    for f, _ in geo._fields_:
-        if f != "reserved" and hasattr(p, f):
-            setattr(p, f, getattr(geo, f))
-    return p
 
 
 @pytest.fixture(scope="module")

@@ -260,3 +260,35 @@ def test_write_outputs(require_gpu, tmp_path):
         with pytest.raises(hb.Fd2Error) as ei:
             t.write_outputs(str(tmp_path))
         assert ei.value.status == 11
+
+
+def test_wall_root_fp64_fallback(require_gpu):
+    """The column-wall quadratic near tangency: the discriminant b^2 - 4ac
+    nearly cancels, and in float its sign -- root or no root -- is noise.
+    The walk recomputes it from the float coefficients in FP64 (products of
+    floats are exact there); compare with an FP64 root of the same float
+    coefficients."""
+    import ctypes
+
+    rng = np.random.default_rng(12)
+    n = 20000
+    qa = rng.uniform(0.2, 1.0, n).astype(np.float32)
+    qb = (rng.uniform(0.5, 10.0, n) * rng.choice([-1.0, 1.0], n)).astype(np.float32)
+    delta = 10.0 ** rng.uniform(-9.5, -5.0, n) * rng.choice([-1.0, 1.0], n)
+    qc = (qb.astype(np.float64) ** 2 / (4.0 * qa.astype(np.float64)) * (1.0 - delta)).astype(np.float32)
+    out = np.zeros(n, np.float32)
+    lib = hb.load()
+    st = lib.fd2_debug_wall_root(n, qa.ctypes.data_as(ctypes.c_void_p), qb.ctypes.data_as(ctypes.c_void_p),
+                                 qc.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p))
+    assert st == 0
+    a, b, c = qa.astype(np.float64), qb.astype(np.float64), qc.astype(np.float64)
+    disc = b * b - 4.0 * a * c
+    s = np.sqrt(np.maximum(disc, 0.0))
+    root = np.where(b >= 0.0, -2.0 * c / (b + s), (s - b) / (2.0 * a))
+    naive = qb * qb - np.float32(4.0) * qa * qc  # the float discriminant without the fallback
+    flipped = np.sign(naive) != np.sign(disc)
+    assert flipped.mean() > 0.1  # the cases do reach the cancellation
+    has = disc >= 0.0
+    assert np.array_equal(out == 999.0, ~has)
+    rel = np.abs(out[has] - root[has]) / np.abs(root[has])
+    assert rel.max() < 1e-5, rel.max()

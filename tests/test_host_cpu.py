@@ -266,3 +266,18 @@ def test_fd2run_usage():
     r = subprocess.run([exe, "--xray", os.path.join(GOLDEN, "example_detected.txt"), "--material", "m.mat", inp],
                        capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "BIGS" in r.stderr
+
+
+def test_host_generator_build_equals_product_generator():
+    """bench.py's reference arm builds its event stream with the host-only
+    build of the generator (oracle/_build/libfd2synth.so), so its process maps
+    no product library; the events are the product generator's."""
+    from oracle import pyoracle as po
+
+    for cfg, n in [(0, 50), (1, 200), (4, 100)]:
+        a = po.synth_events_host(cfg, n, 99)
+        b = hb.synth_events(cfg, n, 99)
+        assert a.n == b.n > 0
+        for k in ("x_um", "y_um", "z_um", "e_ev", "hist"):
+            assert np.array_equal(getattr(a, k), getattr(b, k)), (cfg, k)
+        assert bytes(a.params) == bytes(b.params)

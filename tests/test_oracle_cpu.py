@@ -137,3 +137,24 @@ def test_phs_binning_rules():
     assert list(h) == [3, 0, 1, 0]
     with pytest.raises(ValueError):
         po.phs(np.array([1], np.int32), 0, 5, 10)
+
+
+def test_threaded_oracle_equals_one_call():
+    """The GPU parity tests run the oracle over event slices on host threads
+    (tests/gpu_helpers.run_oracle_parallel); the sums equal one call, and the
+    per-thread call counters of the calling thread are untouched by the
+    workers."""
+    import hybridmantis_b200 as hb
+    from tests.gpu_helpers import run_oracle_on, run_oracle_parallel
+
+    es = hb.synth_events(1, 40, 5)
+    rng = np.random.default_rng(1)
+    N = rng.poisson(es.e_ev.astype(np.float64) * 0.01).astype(np.int32)
+    po.reset_call_counts()
+    a = run_oracle_parallel(es, N, workers=4)
+    assert sum(po.call_counts().values()) == 0
+    b = run_oracle_on(es, N)
+    assert sum(po.call_counts().values()) > 0
+    assert np.array_equal(a.image, b.image)
+    assert np.array_equal(a.per_primary, b.per_primary)
+    assert np.array_equal(a.counters, b.counters)

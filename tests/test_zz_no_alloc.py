@@ -74,3 +74,41 @@ def test_noalloc_rejects_oversized_inputs(require_gpu):
     st = lib.fd2_transport_noalloc(ctypes.byref(geom), dummy, dummy, dummy, dummy, dummy, 262145, 10,
                                    ctypes.c_uint64(1), dummy, dummy, dummy, None)
     assert st == 1
+
+
+@pytest.mark.parametrize("case", ["chunk_overflow", "too_many_photons", "bad_history"])
+def test_noalloc_rejected_call_leaves_tallies(require_gpu, case):
+    """A call the device rejects (more queue chunks than the scratch holds,
+    an event above the 900,000-photon cap, a history outside 1..num_hist)
+    returns its status and adds nothing to the caller's tallies."""
+    import torch
+
+    lib = hb.load()
+    p = hb.default_params(num_hist=1000)
+    geom = hb.params_to_geometry(p)
+    xd, yd = hb.prf_dims(geom)
+    dev = torch.device("cuda", 0)
+    if case == "chunk_overflow":
+        # 600 events x 900,000 photons = 600 x 3,516 chunks of 256 > 2,097,152
+        n, nph, hist, want = 600, np.full(600, 900000, np.int32), np.arange(1, 601, dtype=np.int32), 1
+    elif case == "too_many_photons":
+        n, nph, hist, want = 4, np.array([1000, 900001, 1000, 1000], np.int32), np.arange(1, 5, dtype=np.int32), 6
+    else:
+        n, nph, hist, want = 4, np.full(4, 1000, np.int32), np.array([1, 2, 1001, 3], np.int32), 12
+    pos = torch.full((n,), 250.5, dtype=torch.float32, device=dev)
+    z = torch.full((n,), 10.0, dtype=torch.float32, device=dev)
+    h = torch.from_numpy(hist).to(dev)
+    k = torch.from_numpy(nph).to(dev)
+    prf = torch.zeros(xd * yd, dtype=torch.int64, device=dev)
+    prim = torch.zeros(p.num_hist, dtype=torch.int32, device=dev)
+    cnt = torch.zeros(9, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    torch.cuda.synchronize()
+    st = lib.fd2_transport_noalloc(ctypes.byref(geom), ctypes.c_void_p(pos.data_ptr()),
+                                   ctypes.c_void_p(pos.data_ptr()), ctypes.c_void_p(z.data_ptr()),
+                                   ctypes.c_void_p(h.data_ptr()), ctypes.c_void_p(k.data_ptr()), n, p.num_hist,
+                                   ctypes.c_uint64(7), ctypes.c_void_p(prf.data_ptr()),
+                                   ctypes.c_void_p(prim.data_ptr()), ctypes.c_void_p(cnt.data_ptr()),
+                                   ctypes.c_void_p(stream))
+    assert st == want
+    assert int(cnt.abs().sum()) == 0 and int(prf.abs().sum()) == 0 and int(prim.abs().sum()) == 0
