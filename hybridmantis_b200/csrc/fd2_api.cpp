@@ -205,7 +205,6 @@ fd2_status check_status(fd2_ctx *c)
     if (st & fd2::kStatusTooManyPhotons) return fail(c, FD2_ERR_TOO_MANY_PHOTONS, "an event exceeds max_photons_per_event");
     if (st & fd2::kStatusChunkOverflow) return fail(c, FD2_ERR_OUT_OF_MEMORY, "work-queue capacity exceeded");
     if (st & fd2::kStatusAborted) return fail(c, FD2_ERR_DEVICE_ABORT, "transport aborted");
-    if (st & fd2::kStatusRngUnderflow) return fail(c, FD2_ERR_DEVICE_ABORT, "uniform ring underflow in the walk");
     return FD2_OK;
 }
 

@@ -6,14 +6,14 @@
 // boundary_analysis :1582, transmit :2421, refl_bottom :2985,
 // trans_dir_cos :3169, RoughSurface :3261) decision for decision, with
 // changes that keep the distribution and suit sm_100a:
-//   * every uniform comes from Philox keyed by the run seed at counter
-//     (block, photon-in-event, event, run), so a photon's walk does not
-//     depend on which lane runs it or when;
-//   * uniforms are generated four at a time into a 32-entry per-lane ring in
-//     shared memory, so the walk's draw sites are a shared-memory load, not
-//     an inlined Philox; whenever one lane of the warp must generate, every
-//     lane with room generates too, so the Philox rounds run with most of
-//     the warp instead of the few lanes whose rings happen to be low;
+//   * each photon draws from its own xoshiro128+ stream (Blackman & Vigna,
+//     "Scrambled linear pseudorandom number generators", ACM TOMS 47(4),
+//     2021) whose 128-bit state is one Philox-4x32-10 block (Salmon et al.,
+//     "Parallel random numbers: as easy as 1, 2, 3", SC'11) keyed by the run
+//     seed at counter (0, photon-in-event, event, run): a photon's walk does
+//     not depend on which lane runs it or when, and a draw costs a handful
+//     of integer operations in registers instead of a Philox block per four
+//     uniforms;
 //   * angle tests are made on cosines (acos(c) > 1.57 <=> c < cos 1.57) and
 //     the Fresnel coefficients use the cosine forms, so the walk needs no
 //     acos/asin/tan/pow; the refraction keeps the reference's formula
@@ -67,10 +67,6 @@ __device__ __forceinline__ float u01(uint32_t r)
     return __uint_as_float(0x3F800000u | (r >> 9)) - 0.99999994039535522461f;
 }
 
-constexpr int kURing = 32;      // uniforms buffered per lane
-constexpr int kURingLow = 12;  // inside a step: a lane at or below this level must generate
-constexpr int kURingStep = 24; // the round's refill generates while a lane is at or below this
-
 // Internal step result: the photon waits at a column wall for the Fresnel
 // part of its surface interaction (not a fate).
 constexpr int kNeedsFresnel = 100;
@@ -80,8 +76,8 @@ constexpr int kNeedsFresnel = 100;
 constexpr int kNeedsNormal = 101;
 constexpr int kRetryNormal = 102;
 
-// Warp-uniform part of a Philox stream: the round keys of the run seed
-// (the kernel keeps them in shared memory) and the run counter.
+// Warp-uniform part of a photon's seed: the Philox round keys of the run
+// seed (the kernel keeps them in shared memory) and the run counter.
 struct RngKey {
     const uint32_t *rk;
     uint32_t run;
@@ -127,28 +123,6 @@ __device__ __forceinline__ float wall_root(float qa, float qb, float qc)
     return (s - qb) / (2.0f * qa);
 }
 
-struct RefillState {
-    uint32_t tail, block;
-};
-
-// Refill inside a step: rarely taken once the round's refill leaves every ring
-// above kURingStep, so it is one out-of-line copy instead of an inlined
-// Philox at every loop of the walk (the walk's code then stays small enough
-// for the instruction cache).  Fills the lane's ring completely.
-__device__ __noinline__ RefillState refill_slow(float *ring, int stride, uint32_t head, uint32_t tail, uint32_t block,
-                                               uint32_t photon, uint32_t event, uint32_t run, const uint32_t *rk)
-{
-    while (tail - head <= (uint32_t)(kURing - 4)) {
-        const uint4 r = philox4x32_10_rk(make_uint4(block++, photon, event, run), rk);
-        ring[((tail + 0) & (kURing - 1)) * stride] = u01(r.x);
-        ring[((tail + 1) & (kURing - 1)) * stride] = u01(r.y);
-        ring[((tail + 2) & (kURing - 1)) * stride] = u01(r.z);
-        ring[((tail + 3) & (kURing - 1)) * stride] = u01(r.w);
-        tail += 4;
-    }
-    return {tail, block};
-}
-
 struct Walker {
     // photon
     float px, py, pz;   // position
@@ -160,68 +134,39 @@ struct Walker {
     float budget;       // absorption lengths left before bulk absorption
     uint32_t rebound;   // boundary interactions
     int ii, jj;         // detection pixel (-1: outside the PRF bounds)
-    // Philox stream of the photon and the lane's uniform ring.  Once per
-    // round of the transport loop, after the steps, the warp tops the ring of
-    // every lane whose photon goes on up above kURingStep (top_up, one
-    // inlined copy for the whole round: crosstalk attempts, parked lanes and
-    // the next step alike); at the start of a step and at every loop
-    // iteration and new-normal attempt inside one, a ring at or below
-    // kURingLow is refilled out of line (top_up_inner).  No segment
-    // between two checks draws more than 7, so a draw is a plain
-    // shared-memory load.  `underflow` records a draw from an empty ring
-    // (never expected; reported).  Generating ahead does not change the
-    // values a photon draws: its stream is consumed in counter order.
-    float *ring;
-    int stride;
-    uint32_t head, tail, block, photon, event;
-    RngKey key;
-    bool underflow;
+    // The photon's random stream: xoshiro128+ state (never all zero; a
+    // Philox block is all zero with probability 2^-128, and start() then
+    // sets one bit).  The float uses the top 23 bits of each output, the
+    // bits the generator's authors recommend for floating point.
+    uint32_t s0, s1, s2, s3;
 
-    __device__ __forceinline__ void top_up()
-    {
-        const unsigned mask = __activemask();
-#pragma unroll 1
-        while (__any_sync(mask, tail - head <= (uint32_t)kURingStep)) {
-            if (tail - head <= (uint32_t)(kURing - 4)) {
-                const uint4 r = philox4x32_10_rk(make_uint4(block++, photon, event, key.run), key.rk);
-                ring[((tail + 0) & (kURing - 1)) * stride] = u01(r.x);
-                ring[((tail + 1) & (kURing - 1)) * stride] = u01(r.y);
-                ring[((tail + 2) & (kURing - 1)) * stride] = u01(r.z);
-                ring[((tail + 3) & (kURing - 1)) * stride] = u01(r.w);
-                tail += 4;
-            }
-        }
-    }
-    // Inside a step: keep at least kURingLow + 1 uniforms (no segment between
-    // two calls draws more than 7).
-    __device__ __forceinline__ void top_up_inner()
-    {
-        if (tail - head <= (uint32_t)kURingLow) {
-            const RefillState r = refill_slow(ring, stride, head, tail, block, photon, event, key.run, key.rk);
-            tail = r.tail;
-            block = r.block;
-        }
-    }
     __device__ __forceinline__ float u()
     {
-        underflow |= head == tail;
-        return ring[((head++) & (kURing - 1)) * stride];
+        const uint32_t r = s0 + s3;
+        const uint32_t t = s1 << 9;
+        s2 ^= s0;
+        s3 ^= s1;
+        s1 ^= s2;
+        s0 ^= s3;
+        s2 ^= t;
+        s3 = __funnelshift_l(s3, s3, 11);
+        return u01(r);
     }
 
-    __device__ __forceinline__ void start(uint32_t photon_in_event, uint32_t event_index, bool first)
+    __device__ __forceinline__ void start(uint32_t photon_in_event, uint32_t event_index, bool first,
+                                          const RngKey &key)
     {
-        photon = photon_in_event;
-        event = event_index;
-        block = 0;
-        head = tail = 0;
-        underflow = false;
+        const uint4 k = philox4x32_10_rk(make_uint4(0u, photon_in_event, event_index, key.run), key.rk);
+        s0 = k.x;
+        s1 = k.y;
+        s2 = k.z;
+        s3 = k.w | ((k.x | k.y | k.z | k.w) == 0u ? 1u : 0u);
         px = ex; py = ey; pz = ez;
         xc = ex; yc = ey;
         nx = 0.0f; ny = 0.0f; nz = 0.0f;
         dist = 0.0f;
         rebound = 0;
         ii = -1; jj = -1;
-        top_up();
         emit(first);
         budget = -__logf(u());  // Exp(1)
     }
@@ -232,10 +177,7 @@ struct Walker {
     {
         float c = 2.0f * u() - 1.0f;
         if (first) {
-            for (int t = 0; t < 64 && fabsf(c) <= 0.01f; ++t) {
-                top_up_inner();
-                c = 2.0f * u() - 1.0f;
-            }
+            for (int t = 0; t < 64 && fabsf(c) <= 0.01f; ++t) c = 2.0f * u() - 1.0f;
         }
         const float rr = sqrtf(fmaxf(0.0f, 1.0f - c * c));
         float s, co;
@@ -356,7 +298,6 @@ struct Walker {
                                                      bool always_rough)
     {
         for (;;) {
-            top_up_inner();
             nx = ix; ny = iy; nz = iz;
             roughen(1.0f);
             const float inv = rsqrtf(nx * nx + ny * ny);
@@ -410,7 +351,6 @@ struct Walker {
         int tries = 0, tries_top = 0;
         bool side_hop = true;
         for (int loop = 0; loop < kMaxTopLoops; ++loop) {
-            top_up_inner();
             bool sensor_hit = false;
             {
                 const float sx = px, sy = py, sz = pz;
@@ -463,7 +403,6 @@ struct Walker {
             // top reflector / sensor at the end of the hop
             bool again = false;
             for (int k = 0; k < kMaxTopLoops; ++k) {
-                top_up_inner();
                 if (at_top(g)) {
                     if (g.top_absfrac > 0.0f && u() < g.top_absfrac) return kAbsTop;
                     dz = -fabsf(2.0f * u() - 1.0f);
@@ -531,7 +470,6 @@ struct Walker {
     template <class G>
     __device__ __forceinline__ int crosstalk_normal(const G &g, int &tries)
     {
-        top_up_inner();
         const float ix = -dx, iy = -dy, iz = -dz;
         nx = ix; ny = iy; nz = iz;
         roughen(1.0f);
@@ -563,7 +501,6 @@ struct Walker {
         enum { kLeave, kNewSurface, kRestore, kIncidence } stage = kNewSurface;
         int fate = kAlive;
         for (int loop = 0; loop < kMaxSurfaceLoops; ++loop) {
-            top_up_inner();
             if (stage == kNewSurface) {
                 if (!outside) {
                     const float ax = xc - px, ay = yc - py;
@@ -771,7 +708,6 @@ struct Walker {
         const float sgn = inside ? -1.0f : 1.0f;  // normal toward the incident medium
         float c1 = 0.0f;
         for (int t = 0; t < 8; ++t) {
-            top_up_inner();
             nx = sgn * ox; ny = sgn * oy; nz = 0.0f;
             if (g.beta > 0.0f) roughen(g.beta);
             c1 = -(dx * nx + dy * ny + dz * nz);
@@ -968,11 +904,9 @@ struct Walker {
 
     // One segment of the lattice walk: a flight to the next surface and what
     // happens there, the interaction in one place for lanes in either medium.
-    // Draws at most 7 uniforms between ring checks.
     template <class G>
     __device__ __forceinline__ int grid_segment(const G &g)
     {
-        top_up_inner();
         if (++rebound > kMaxBoundaryCalls) return kCapped;
         float wx = 0.0f, wy = 0.0f;
         bool win = false;
@@ -989,7 +923,6 @@ struct Walker {
     template <class G>
     __device__ __forceinline__ int step(const G &g)
     {
-        top_up_inner();  // a step draws at most 6 uniforms; the round's refill follows it
         int f = flight(g);
         if (f != kAlive) return f;
         if (fabsf(pz + g.half) < kEps) {

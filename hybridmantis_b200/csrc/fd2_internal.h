@@ -58,7 +58,7 @@ enum : int {
     kStatusBadEvent = 2,
     kStatusAborted = 4,
     kStatusChunkOverflow = 8,
-    kStatusRngUnderflow = 16  // a walk segment drew more uniforms than buffered
+    kStatusRngUnderflow = 16  // reserved (raised by no kernel since the walk draws in registers)
 };
 
 constexpr int kCounterStride = kNumFates + 1;

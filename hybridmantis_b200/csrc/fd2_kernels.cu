@@ -306,7 +306,7 @@ constexpr int kRing = 32;
 
 // Shared-memory layout of the transport kernel (dynamic).
 struct SmemLayout {
-    size_t geom, ring, cnt, dist, win, uring, total;
+    size_t geom, ring, cnt, dist, win, total;
     __host__ __device__ SmemLayout(int block, int n_geom, int window)
     {
         size_t o = 0;
@@ -322,8 +322,6 @@ struct SmemLayout {
         o = (o + 15) & ~(size_t)15;
         win = o;
         o += sizeof(unsigned) * (size_t)window * window;
-        uring = o;
-        o += sizeof(float) * (size_t)kURing * block;
         total = o;
     }
 };
@@ -352,7 +350,6 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     unsigned int *s_cnt = reinterpret_cast<unsigned int *>(smem + L.cnt);
     float *s_dist = reinterpret_cast<float *>(smem + L.dist);
     unsigned int *s_win = reinterpret_cast<unsigned int *>(smem + L.win);
-    float *s_uring = reinterpret_cast<float *>(smem + L.uring);
     (void)nwarps;
 
     if (kMulti)
@@ -380,10 +377,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
 
     __syncthreads();
     Walker w;
-    w.ring = s_uring + threadIdx.x;
-    w.stride = blockDim.x;
-    w.key.rk = s_rk;
-    w.key.run = s_run;
+    const RngKey key{s_rk, s_run};
     int prim = 0, geom = 0;
 
     for (;;) {
@@ -444,7 +438,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                     w.ex = s.pos.x; w.ey = s.pos.y; w.ez = s.pos.z;
                     prim = __float_as_int(s.pos.w);
                     geom = (int)s.geom;
-                    w.start(k, (uint32_t)(a.event_base + s.event), k == 0);
+                    w.start(k, (uint32_t)(a.event_base + s.event), k == 0, key);
                     if constexpr (kGrid) w.grid_place(a.g0);
                     alive = true;
                 }
@@ -472,7 +466,6 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             const unsigned col = __ballot_sync(kFull, alive && !w.in_gap);
             const bool go = alive && (!w.in_gap || (unsigned)__popc(gap) >= fresnel_min || col == 0);
             if (go) fate = w.grid_segment(a.g0);
-            if (alive && fate == kAlive) w.top_up();
         } else {
             if (alive && !parked && !xretry) {
                 fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
@@ -481,10 +474,6 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                     fate = kAlive;
                 }
             }
-            // one warp-wide refill per round, in one inlined copy, for every lane
-            // whose photon goes on: crosstalk attempts, parked lanes and the next
-            // round's step alike
-            if ((alive && fate == kAlive) || fate == kNeedsNormal) w.top_up();
             if (alive && !parked) {
                 // crosstalk: one attempt at the next column's normal per round, so
                 // a rejected attempt is retried beside the other lanes' first ones
@@ -511,7 +500,6 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         const unsigned ended = __ballot_sync(kFull, fate != kAlive);
         if (ended) {
             if (fate != kAlive) {
-                if (w.underflow) atomicOr(a.status, kStatusRngUnderflow);
                 const unsigned key = (unsigned)(geom * kCounterStride + fate);
                 const unsigned peers = __match_any_sync(ended, key);
                 if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[key], (unsigned)__popc(peers));

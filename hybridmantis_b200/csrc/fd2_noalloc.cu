@@ -232,6 +232,6 @@ extern "C" fd2_status fd2_transport_noalloc(const fd2_geometry *geometry, const 
     if (status & fd2::kStatusBadEvent) return FD2_ERR_BAD_EVENT;
     if (status & fd2::kStatusTooManyPhotons) return FD2_ERR_TOO_MANY_PHOTONS;
     if (status & fd2::kStatusChunkOverflow) return FD2_ERR_INVALID_ARGUMENT;  // more photons than the scratch holds
-    if (status & (fd2::kStatusAborted | fd2::kStatusRngUnderflow)) return FD2_ERR_DEVICE_ABORT;
+    if (status & fd2::kStatusAborted) return FD2_ERR_DEVICE_ABORT;
     return FD2_OK;
 }
