@@ -15,6 +15,7 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include <dlfcn.h>
@@ -368,6 +369,31 @@ void fit_window(fd2_ctx *c)
     }
 }
 
+// Launch shape unless the options give one, measured on a B200 (config-1
+// events, 20,000 x-rays): one geometry 256 threads x 4 CTAs per SM (32 warps
+// at 64 registers; 6.7e8 photons/s against 5.8e8 for 320 x 2), chunks of 16
+// photons; several geometries 256 x 3 (8.5e8 against 7.9e8 for 256 x 4,
+// whose variant spills); the column lattice 320 x 2 (2.2e8 against 2.0e8 for
+// 256 x 2 or x 3); label mode 256 x 2 (its only variant).
+static void default_launch(const fd2_ctx *c, int n_geom, fd2::TransportConfig *cfg)
+{
+    int block = 256, ctas = 4, chunk = 16;
+    if (c->opt.radial_bins > 0) {
+        ctas = 2;
+        chunk = 32;
+    } else if (c->opt.column_grid) {
+        block = 320;
+        ctas = 2;
+        chunk = 32;
+    } else if (n_geom > 1) {
+        ctas = 3;
+        chunk = 32;
+    }
+    cfg->block = c->opt.block_size > 0 ? c->opt.block_size : block;
+    cfg->ctas_per_sm = c->opt.ctas_per_sm > 0 ? c->opt.ctas_per_sm : ctas;
+    cfg->chunk = c->opt.chunk > 0 ? c->opt.chunk : chunk;
+}
+
 fd2_status set_config(fd2_ctx *c, const fd2::TransportConfig &cfg)
 {
     fd2::TransportConfig k = cfg;
@@ -606,10 +632,7 @@ fd2_status fd2_create(const fd2_params *p, const fd2_options *opt, fd2_ctx **out
     c->geoms.assign(1, g);
     if ((st = alloc_tallies(c)) != FD2_OK) return bail(st);
     fd2::TransportConfig cfg;
-    // defaults: what the autotuner picks for the config-1 workload on a B200
-    cfg.block = c->opt.block_size > 0 ? c->opt.block_size : (c->opt.radial_bins > 0 ? 256 : 320);  // label mode: 256
-    cfg.ctas_per_sm = c->opt.ctas_per_sm > 0 ? c->opt.ctas_per_sm : 2;
-    cfg.chunk = c->opt.chunk > 0 ? c->opt.chunk : 32;
+    default_launch(c, 1, &cfg);
     cfg.refill = c->opt.refill > 0 ? c->opt.refill : 4;
     // parked lanes before the warp's Fresnel pass (8), or with a column lattice
     // gap lanes before the warp's gap segments (12: square 1.755 / hexagonal
@@ -675,7 +698,9 @@ fd2_status fd2_set_geometries(fd2_ctx *c, const fd2_geometry *g, int32_t n)
     c->counts_ready = false;
     fd2_status st = alloc_tallies(c);
     if (st != FD2_OK) return st;
-    return set_config(c, c->cfg);
+    fd2::TransportConfig k = c->cfg;
+    default_launch(c, n, &k);
+    return set_config(c, k);
 }
 
 // What every submission does once the events are on the device: the PRF
@@ -1206,37 +1231,45 @@ fd2_status fd2_autotune(fd2_ctx *c, int32_t budget_runs)
     float best_ms = 0.0f;
     if ((st = time_cfg(best, &best_ms)) != FD2_OK) return st;
     int runs = 2;
-    const std::vector<int> blocks = {128, 256, 320, 384, 512};
-    const std::vector<int> ctas = {1, 2, 3, 4};
+    // launch shapes as (threads per CTA, CTAs per SM) pairs -- the register
+    // budget of each compiled variant ties the two together -- then chunk,
+    // refill and Fresnel batch one knob at a time, twice over
+    const std::vector<std::pair<int, int>> shapes = {{256, 4}, {128, 8}, {256, 3}, {320, 2}, {256, 2}, {512, 1}};
     const std::vector<int> chunks = {8, 16, 32, 64, 128};
-    const std::vector<int> refills = {1, 4, 8, 16};
-    const std::vector<int> fresnels = {1, 4, 8, 16};
+    const std::vector<int> refills = {1, 2, 4, 8, 16};
+    const std::vector<int> fresnels = {1, 4, 8, 12, 16};
+    auto try_cfg = [&](const fd2::TransportConfig &k) {
+        // the CTA's shared memory must fit ctas_per_sm times (set_config
+        // shrinks the PRF window to fit; without it, skip)
+        fd2::TransportConfig bare = k;
+        bare.window = 0;
+        if (fd2::transport_smem_bytes(bare, (int)c->geoms.size()) * (size_t)k.ctas_per_sm > 220 * 1024) return;
+        float ms = 0.0f;
+        if (time_cfg(k, &ms) != FD2_OK) return;
+        runs += 2;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = k;
+        }
+    };
     for (int pass = 0; pass < 2; ++pass) {
-        for (int knob = 0; knob < 5; ++knob) {
-            const std::vector<int> &vals =
-                knob == 0 ? blocks : knob == 1 ? ctas : knob == 2 ? chunks : knob == 3 ? refills : fresnels;
+        for (const auto &sh : shapes) {
+            if (budget_runs > 0 && runs >= budget_runs) break;
+            if (sh.first == best.block && sh.second == best.ctas_per_sm) continue;
+            fd2::TransportConfig k = best;
+            k.block = sh.first;
+            k.ctas_per_sm = sh.second;
+            try_cfg(k);
+        }
+        for (int knob = 0; knob < 3; ++knob) {
+            const std::vector<int> &vals = knob == 0 ? chunks : knob == 1 ? refills : fresnels;
             for (int v : vals) {
                 if (budget_runs > 0 && runs >= budget_runs) break;
                 fd2::TransportConfig k = best;
-                int &slot = knob == 0 ? k.block
-                            : knob == 1 ? k.ctas_per_sm
-                            : knob == 2 ? k.chunk
-                            : knob == 3 ? k.refill
-                                        : k.fresnel;
+                int &slot = knob == 0 ? k.chunk : knob == 1 ? k.refill : k.fresnel;
                 if (slot == v) continue;
                 slot = v;
-                // the CTA's shared memory must fit ctas_per_sm times (set_config
-                // shrinks the PRF window to fit; without it, skip)
-                fd2::TransportConfig bare = k;
-                bare.window = 0;
-                if (fd2::transport_smem_bytes(bare, (int)c->geoms.size()) * (size_t)k.ctas_per_sm > 220 * 1024) continue;
-                float ms = 0.0f;
-                if (time_cfg(k, &ms) != FD2_OK) continue;
-                runs += 2;
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = k;
-                }
+                try_cfg(k);
             }
         }
     }

@@ -129,7 +129,6 @@ struct Walker {
     float dx, dy, dz;   // direction
     float nx, ny, nz;   // current surface normal
     float xc, yc;       // centre of the current column
-    float ex, ey, ez;   // emission point (the event)
     float dist;         // path length
     float budget;       // absorption lengths left before bulk absorption
     uint32_t rebound;   // boundary interactions
@@ -153,8 +152,12 @@ struct Walker {
         return u01(r);
     }
 
-    __device__ __forceinline__ void start(uint32_t photon_in_event, uint32_t event_index, bool first,
-                                          const RngKey &key)
+    // Start photon `photon_in_event` of event `event_index` at the event's
+    // position (ex, ey, ez), in the column centred on it.  The event record
+    // itself stays outside the walker (the kernel keeps it in shared memory),
+    // so it holds no registers through the walk.
+    __device__ __forceinline__ void start(float ex, float ey, float ez, uint32_t photon_in_event,
+                                          uint32_t event_index, bool first, const RngKey &key)
     {
         const uint4 k = philox4x32_10_rk(make_uint4(0u, photon_in_event, event_index, key.run), key.rk);
         s0 = k.x;
@@ -226,7 +229,6 @@ struct Walker {
     template <class G>
     __device__ __forceinline__ int flight(const G &g)
     {
-        if (rebound == 0) { xc = ex; yc = ey; }
         const float ddx = px - xc, ddy = py - yc;
         const float qa = dx * dx + dy * dy;
         const float qb = 2.0f * (ddx * dx + ddy * dy);
@@ -917,11 +919,11 @@ struct Walker {
     }
 
     // One transport step (the body of the reference's step function algo):
-    // flight, sensor, trapped-photon restart, or a surface interaction up to
-    // the Fresnel part.  Returns the photon's fate, kAlive while it is in
+    // flight, sensor, trapped-photon restart (from `event`, the x, y, z of
+    // the photon's event), or a surface interaction up to the Fresnel part.  Returns the photon's fate, kAlive while it is in
     // flight, or kNeedsFresnel (run surface_fresnel next).
     template <class G>
-    __device__ __forceinline__ int step(const G &g)
+    __device__ __forceinline__ int step(const G &g, const float4 &event)
     {
         int f = flight(g);
         if (f != kAlive) return f;
@@ -939,7 +941,7 @@ struct Walker {
         if (fabsf(dz) < kEps) {
             // trapped travelling horizontally: restart from the event position,
             // keeping the current column (the reference does not reset it)
-            px = ex; py = ey; pz = ez;
+            px = event.x; py = event.y; pz = event.z;
             emit(false);
             return kAlive;
         }

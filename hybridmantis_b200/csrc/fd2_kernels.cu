@@ -378,7 +378,13 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     __syncthreads();
     Walker w;
     const RngKey key{s_rk, s_run};
-    int prim = 0, geom = 0;
+    int geom = 0;
+    // the lane's current event record (x, y, z, history index bits): read at
+    // a trapped restart, a detection and in label mode, so it need not stay
+    // in registers through the walk; and the lane's path-length sum
+    __shared__ float4 s_lane[kMaxThreads];
+    __shared__ float s_ldist[kMaxThreads];
+    s_ldist[threadIdx.x] = 0.0f;
 
     for (;;) {
         // ---- hand out photons to idle lanes
@@ -435,10 +441,9 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                 if (mine) {
                     const Slot &s = ring[slot];
                     const uint32_t k = s.first + used + rank;
-                    w.ex = s.pos.x; w.ey = s.pos.y; w.ez = s.pos.z;
-                    prim = __float_as_int(s.pos.w);
+                    s_lane[threadIdx.x] = s.pos;
                     geom = (int)s.geom;
-                    w.start(k, (uint32_t)(a.event_base + s.event), k == 0, key);
+                    w.start(s.pos.x, s.pos.y, s.pos.z, k, (uint32_t)(a.event_base + s.event), k == 0, key);
                     if constexpr (kGrid) w.grid_place(a.g0);
                     alive = true;
                 }
@@ -468,7 +473,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             if (go) fate = w.grid_segment(a.g0);
         } else {
             if (alive && !parked && !xretry) {
-                fate = kMulti ? w.step(s_geom[geom]) : w.step(a.g0);
+                fate = kMulti ? w.step(s_geom[geom], s_lane[threadIdx.x]) : w.step(a.g0, s_lane[threadIdx.x]);
                 if (fate == kNeedsFresnel) {
                     parked = true;
                     fate = kAlive;
@@ -503,18 +508,21 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                 const unsigned key = (unsigned)(geom * kCounterStride + fate);
                 const unsigned peers = __match_any_sync(ended, key);
                 if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[key], (unsigned)__popc(peers));
-                atomicAdd(&s_dist[geom], w.dist);
+                if (kMulti) atomicAdd(&s_dist[geom], w.dist);
+                else s_ldist[threadIdx.x] += w.dist;  // lane-private: no atomic
                 alive = false;
             }
             const unsigned det = __ballot_sync(kFull, fate == kDetect);
             if (fate == kDetect) {
+                const float4 ev = s_lane[threadIdx.x];
+                const int prim = __float_as_int(ev.w);
                 const unsigned peers = __match_any_sync(det, prim);
                 if (lane == __ffs(peers) - 1 && (unsigned)prim < (unsigned)a.n_prim)
                     atomicAdd(&a.per_primary[prim], __popc(peers));
                 const int xdim = kMulti ? s_geom[geom].xdim : a.g0.xdim;
                 const int ydim = kMulti ? s_geom[geom].ydim : a.g0.ydim;
                 if (kRadial) {
-                    const float rx = w.px - w.ex, ry = w.py - w.ey;
+                    const float rx = w.px - ev.x, ry = w.py - ev.y;
                     // quadratic edges: bin = floor(bins sqrt(r / r_max))
                     const float rr = sqrtf(rx * rx + ry * ry) * a.radial_inv_max;
                     const int b = rr < 1.0f ? min((int)(sqrtf(rr) * (float)a.radial_bins), a.radial_bins - 1)
@@ -539,6 +547,13 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
     __syncthreads();
     for (int i = threadIdx.x; i < a.n_geom * kCounterStride; i += blockDim.x)
         if (s_cnt[i]) atomicAdd(&a.counters[i], (unsigned long long)s_cnt[i]);
+    if (!kMulti) {
+        // the lanes' path-length sums: summed per warp in double, then added to the CTA's
+        double d = (double)s_ldist[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+        if (lane == 0 && d != 0.0) atomicAdd(&a.distance[0], d);
+    }
     for (int i = threadIdx.x; i < a.n_geom; i += blockDim.x)
         if (s_dist[i] != 0.0f) atomicAdd(&a.distance[i], (double)s_dist[i]);
     if (win > 0) {
@@ -692,7 +707,8 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
     X(false, 256, 2, false, true) X(false, 320, 2, false, true)          \
     X(false, 256, 3, false, false) X(false, 256, 4, false, false)        \
     X(true, 512, 1, false, false) X(true, 256, 2, false, false)          \
-    X(true, 256, 3, false, false) X(true, 256, 2, true, false)
+    X(true, 256, 3, false, false) X(true, 256, 2, true, false)          \
+    X(true, 256, 4, false, false) X(false, 256, 3, false, true)
 
 cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
 {
@@ -730,11 +746,12 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
     const size_t smem = transport_smem_bytes(cfg, a.n_geom);
     const unsigned grid = (unsigned)(sm_count * cfg.ctas_per_sm);
     const bool multi = a.n_geom > 1;
-    const int per_sm = cfg.block > 256 ? 1 : std::min(std::max(cfg.ctas_per_sm, 2), multi ? 3 : 4);
+    const int per_sm = cfg.block > 256 ? 1 : std::min(std::max(cfg.ctas_per_sm, 2), 4);
     if (a.g0.grid) {
         // explicit column lattice: single geometry, 256 or 320 threads
         if (multi || a.radial) return cudaErrorInvalidConfiguration;
         if (cfg.block == 320) transport_kernel<false, 320, 2, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else if (cfg.block <= 256 && per_sm >= 3) transport_kernel<false, 256, 3, false, true><<<grid, cfg.block, smem, s>>>(a);
         else if (cfg.block <= 256) transport_kernel<false, 256, 2, false, true><<<grid, cfg.block, smem, s>>>(a);
         else return cudaErrorInvalidConfiguration;
     } else if (a.radial) {
@@ -751,7 +768,8 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
         if (cfg.block == 320) transport_kernel<true, 320, 2><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 1) transport_kernel<true, 512, 1><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 2) transport_kernel<true, 256, 2><<<grid, cfg.block, smem, s>>>(a);
-        else transport_kernel<true, 256, 3><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 3) transport_kernel<true, 256, 3><<<grid, cfg.block, smem, s>>>(a);
+        else transport_kernel<true, 256, 4><<<grid, cfg.block, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
