@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
         ("prf_window", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("wait_timeout_s", ctypes.c_double),
         ("tune_cache", ctypes.c_char_p), ("event_base", ctypes.c_int64), ("fresnel_batch", ctypes.c_int32),
         ("radial_bins", ctypes.c_int32), ("radial_max_um", ctypes.c_double),
-        ("column_grid", ctypes.c_int32), ("grid_gap_um", ctypes.c_double),
+        ("column_grid", ctypes.c_int32), ("grid_gap_um", ctypes.c_double), ("tally_mode", ctypes.c_int32),
     ]
 
 

@@ -219,6 +219,7 @@ void choose_window_sums(fd2_ctx *c, double sx, double sy, int64_t k)
     int w = c->opt.prf_window;
     if (w < 0) w = 128;
     if (c->d_radial) w = 0;  // label mode tallies no PRF image
+    if (c->opt.tally_mode == 0) w = 0;  // per-lane reductions go straight to the global PRF
     if (w > g.xdim) w = g.xdim;
     if (w > g.ydim) w = g.ydim;
     if (w > 176) w = 176;  // fits beside the rings in shared memory
@@ -274,6 +275,7 @@ fd2::TransportArgs transport_args(fd2_ctx *c)
     a.refill = c->cfg.refill;
     a.fresnel_batch = c->cfg.fresnel;
     a.window = c->cfg.window;
+    a.tally_direct = c->opt.tally_mode == 0 ? 1 : 0;
     a.win_x0 = c->win_x0;
     a.win_y0 = c->win_y0;
     a.abort_flag = c->d_abort;

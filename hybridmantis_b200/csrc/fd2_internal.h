@@ -43,6 +43,7 @@ struct TransportArgs {
     int refill;
     int fresnel_batch;           // parked lanes before the Fresnel pass runs
     int window;                  // window edge (0 = off), applies to geometry 0
+    int tally_direct;            // 1: per-lane global reductions; 0: warp-aggregated, shared-memory privatised
     int win_x0, win_y0;          // window origin in pixels
     const volatile int *abort_flag;
     int *status;

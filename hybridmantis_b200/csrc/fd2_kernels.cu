@@ -330,9 +330,11 @@ struct SmemLayout {
 // shared memory, filled with one coalesced load per lane; each lane owns one
 // photon at a time and takes a new one from the ring as soon as (or, with
 // refill > 1, once enough lanes of the warp are) idle, so lanes never wait
-// for the longest walk in the warp.  Fates, per-primary counts and PRF
-// pixels are aggregated across the warp before touching memory; the PRF
-// core of geometry 0 is tallied in a shared-memory window.  kMulti: the
+// for the longest walk in the warp.  Tallies: by default every ended photon
+// adds to the global fates, per-primary counts and PRF with one L2
+// reduction of its lane; with tally_direct = 0 they are aggregated across
+// the warp before touching memory and the PRF core of geometry 0 is tallied
+// in a shared-memory window (identical tallies, slower on a B200).  kMulti: the
 // geometry of each photon comes from the table in shared memory; otherwise
 // the single geometry is read from the kernel parameters.  kRadial (label
 // mode): a detected photon is binned by its distance from its event into
@@ -501,13 +503,19 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             }
         }
 
-        // ---- warp-aggregated tallies of the photons that ended
+        // ---- tallies of the photons that ended: one global reduction per lane
+        // (tally_direct), or aggregated across the warp and privatised in
+        // shared memory
         const unsigned ended = __ballot_sync(kFull, fate != kAlive);
         if (ended) {
             if (fate != kAlive) {
                 const unsigned key = (unsigned)(geom * kCounterStride + fate);
-                const unsigned peers = __match_any_sync(ended, key);
-                if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[key], (unsigned)__popc(peers));
+                if (a.tally_direct) {
+                    atomicAdd(&a.counters[key], 1ull);
+                } else {
+                    const unsigned peers = __match_any_sync(ended, key);
+                    if (lane == __ffs(peers) - 1) atomicAdd(&s_cnt[key], (unsigned)__popc(peers));
+                }
                 if (kMulti) atomicAdd(&s_dist[geom], w.dist);
                 else s_ldist[threadIdx.x] += w.dist;  // lane-private: no atomic
                 alive = false;
@@ -516,9 +524,13 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             if (fate == kDetect) {
                 const float4 ev = s_lane[threadIdx.x];
                 const int prim = __float_as_int(ev.w);
-                const unsigned peers = __match_any_sync(det, prim);
-                if (lane == __ffs(peers) - 1 && (unsigned)prim < (unsigned)a.n_prim)
-                    atomicAdd(&a.per_primary[prim], __popc(peers));
+                if (a.tally_direct) {
+                    if ((unsigned)prim < (unsigned)a.n_prim) atomicAdd(&a.per_primary[prim], 1);
+                } else {
+                    const unsigned peers = __match_any_sync(det, prim);
+                    if (lane == __ffs(peers) - 1 && (unsigned)prim < (unsigned)a.n_prim)
+                        atomicAdd(&a.per_primary[prim], __popc(peers));
+                }
                 const int xdim = kMulti ? s_geom[geom].xdim : a.g0.xdim;
                 const int ydim = kMulti ? s_geom[geom].ydim : a.g0.ydim;
                 if (kRadial) {
@@ -530,7 +542,8 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                     if ((unsigned)prim < (unsigned)a.n_prim && b >= 0)
                         atomicAdd(&a.radial[(long long)prim * (a.radial_bins + 1) + b], 1u);
                 } else if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {
-                    atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);
+                    if (a.tally_direct) atomicAdd(&a.counters[geom * kCounterStride + kNumFates], 1ull);
+                    else atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);
                     const int wx = w.ii - a.win_x0, wy = w.jj - a.win_y0;
                     if (geom == 0 && win > 0 && (unsigned)wx < (unsigned)win && (unsigned)wy < (unsigned)win) {
                         atomicAdd(&s_win[wx * win + wy], 1u);

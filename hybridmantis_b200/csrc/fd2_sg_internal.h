@@ -21,6 +21,7 @@ constexpr int kOutPad = 64;  // output width of the last GEMM
 constexpr int kMaxSplits = 16;
 constexpr float kMuScale = 50.0f;  // ring radius = kMuScale * softplus(output), um (>= 0)
 constexpr float kSdScale = 10.0f;  // um
+constexpr float kLateralUnitUm = 50.0f;  // unit of feature 2, the deposition's distance from the detector centre
 constexpr float kLogSdMin = -6.0f, kLogSdMax = 4.0f;
 
 // Radial categories: bin j < bins covers [e_j, e_{j+1}) with quadratic edges

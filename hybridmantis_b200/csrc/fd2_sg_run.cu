@@ -13,9 +13,8 @@
 //   5. sampling, one warp per row: detected count ~ Binomial(N, p) split over
 //      the 32 lanes (geometric skipping), then each detected photon's radius
 //      drawn exactly from one ring of the mixture, an azimuth uniform over
-//      the directions that stay on the detector (the labels' depositions sit
-//      at the detector centre, so their far light is what the detector's
-//      edges leave), and the PRF pixel;
+//      the directions that stay on the detector (the labels' far light is
+//      what the detector's edges leave), and the PRF pixel;
 //      per-history counts and counters as the Monte Carlo tallies them;
 //   6. PHS and the run counter (the context's last pipeline segment);
 //   7. audit: the audited rows' depositions are transported by the Monte
@@ -128,7 +127,7 @@ __global__ void route_kernel(const RouteArgs a)
         float f[kFeatures];
         f[0] = g.half - p.z;                 // depth below the entrance surface
         f[1] = (float)(a.ev_e[e] * 1e-3);    // keV
-        f[2] = 0.5f;                          // in-column offset: no effect in the walk
+        f[2] = hypotf(p.x - 0.5f * g.xdet, p.y - 0.5f * g.ydet) * (1.0f / kLateralUnitUm);  // from the centre
         f[3] = g.H;
         f[4] = g.R;
         f[5] = g.beta;

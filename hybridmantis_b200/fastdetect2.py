@@ -163,7 +163,7 @@ class OpticalTransport:
                  use_graph: bool = True, wait_timeout_s: float = 0.0, max_photons_per_event: int = 900000,
                  tune_cache: str | None = None, event_base: int = 0, fresnel_batch: int = 0,
                  radial_bins: int = 0, radial_max_um: float = 200.0, column_grid: int = 0,
-                 grid_gap_um: float = 0.5):
+                 grid_gap_um: float = 0.5, tally_mode: int = 0):
         lib = load()
         self._lib = lib
         opt = Options()
@@ -183,6 +183,7 @@ class OpticalTransport:
         opt.radial_max_um = radial_max_um
         opt.column_grid = column_grid
         opt.grid_gap_um = grid_gap_um
+        opt.tally_mode = tally_mode
         self.radial_bins = radial_bins
         self._tune_cache = tune_cache.encode() if tune_cache else None
         opt.tune_cache = self._tune_cache

@@ -17,12 +17,13 @@ from . import _lib
 from ._lib import Geometry, SgConfig, SgHull, SgStats, check, load, ptr
 from .fastdetect2 import COUNT_GIVEN, OpticalTransport, default_params
 
-FEATURES = ["depth_um", "energy_kev", "offset", "thickness_um", "radius_um", "beta", "top_reflectivity",
+FEATURES = ["depth_um", "energy_kev", "lateral_r", "thickness_um", "radius_um", "beta", "top_reflectivity",
             "log10_mu"]
 N_FEATURES = 8
 N_OUTPUTS = 25
 N_COMPONENTS = 8
 MU_SCALE, SD_SCALE = 50.0, 10.0
+LATERAL_UNIT_UM = 50.0  # unit of feature 2: the deposition's distance from the detector centre
 
 
 def geometry_features(g: Geometry) -> np.ndarray:
@@ -31,13 +32,15 @@ def geometry_features(g: Geometry) -> np.ndarray:
                     np.float32)
 
 
-def features(depth_um, energy_kev, offset, g: Geometry) -> np.ndarray:
+def features(depth_um, energy_kev, lateral_um, g: Geometry) -> np.ndarray:
+    """Network inputs of depositions at depth `depth_um` below the entrance
+    surface, energy `energy_kev`, `lateral_um` from the detector centre."""
     depth_um = np.asarray(depth_um, np.float32)
     n = depth_um.size
     f = np.empty((n, N_FEATURES), np.float32)
     f[:, 0] = depth_um
     f[:, 1] = energy_kev
-    f[:, 2] = offset
+    f[:, 2] = np.asarray(lateral_um, np.float32) / LATERAL_UNIT_UM
     f[:, 3:] = geometry_features(g)
     return f
 
@@ -64,12 +67,14 @@ def sample_geometries(n: int, seed: int, base: Geometry | None = None) -> list:
 
 
 def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: int = 0, radial_bins: int = 96,
-                 radial_max_um: float = 400.0, energy_kev=(1.0, 80.0)):
-    """Monte Carlo labels: for each geometry, `points_per_geom` depositions at
-    the detector centre with depth H u (half of them) or H u^2 (the other
-    half: denser near the entrance surface, where x-rays deposit most and
-    the PRF is widest), u ~ U(0, 1), energy U(energy_kev) and in-column
-    offset U(0, 1), each transported with `photons` photons.  Returns
+                 radial_max_um: float = 400.0, energy_kev=(1.0, 80.0), lateral_um: float = 60.0):
+    """Monte Carlo labels: for each geometry, `points_per_geom` depositions
+    with depth H u (half of them) or H u^2 (the other half: denser near the
+    entrance surface, where x-rays deposit most and the PRF is widest),
+    u ~ U(0, 1), energy U(energy_kev), placed uniformly over the disc of
+    radius `lateral_um` around the detector centre (the detected fraction
+    falls with the distance from the centre, as photons reach the detector's
+    sides), each transported with `photons` photons.  Returns
     (features [n, 8], photons [n], detected [n], radial [n, radial_bins + 1])."""
     rng = np.random.default_rng(seed)
     feats, phot, det, rad = [], [], [], []
@@ -85,11 +90,15 @@ def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: i
             u = rng.uniform(0.001, 0.999, n)
             u = np.where(rng.random(n) < 0.5, u, np.maximum(u * u, 0.001))
             depth = (H * u).astype(np.float32).astype(np.float64)
-            cx = np.array([g.det_x / 2.0 for g in gs])[gi]
-            cy = np.array([g.det_y / 2.0 for g in gs])[gi]
+            lat = lateral_um * np.sqrt(rng.uniform(0.0, 1.0, n))
+            phi = rng.uniform(0.0, 2.0 * np.pi, n)
+            cx = (np.array([g.det_x / 2.0 for g in gs])[gi] + lat * np.cos(phi)).astype(np.float32)
+            cy = (np.array([g.det_y / 2.0 for g in gs])[gi] + lat * np.sin(phi)).astype(np.float32)
+            # the feature is the distance of the float positions the walk starts from
+            lat = np.hypot(cx.astype(np.float64) - np.array([g.det_x / 2.0 for g in gs])[gi],
+                           cy.astype(np.float64) - np.array([g.det_y / 2.0 for g in gs])[gi])
             z = H / 2.0 - depth
             energy = rng.uniform(energy_kev[0], energy_kev[1], n)
-            offset = rng.uniform(0.0, 1.0, n)
             nph = np.full(n, photons, np.int32)
             t.submit_events_um(cx, cy, z, energy * 1000.0, np.arange(1, n + 1), nphot=nph, geom=gi)
             t.run_sync()
@@ -98,7 +107,7 @@ def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: i
         f = np.empty((n, N_FEATURES), np.float32)
         f[:, 0] = depth
         f[:, 1] = energy
-        f[:, 2] = offset
+        f[:, 2] = lat / LATERAL_UNIT_UM
         f[:, 3:] = np.stack([geometry_features(g) for g in gs])[gi]
         feats.append(f)
         phot.append(nph)

@@ -146,6 +146,15 @@ typedef struct fd2_options {
                                       counterpart in the reference; single
                                       geometry, production transport only)  */
     double grid_gap_um;            /* lattice: gap between neighbouring columns */
+    int32_t tally_mode;            /* 0 (default): each ended photon adds to the
+                                      global tallies with one L2 reduction of its
+                                      lane; 1: fates and per-history counts are
+                                      aggregated across the warp (__match_any_sync)
+                                      and privatised in shared memory, the PRF core
+                                      in a shared-memory window (prf_window).  The
+                                      tallies are identical; 0 is faster on a B200
+                                      (the tally rate is far below the L2's atomic
+                                      throughput, so aggregation only costs issue) */
 } fd2_options;
 
 typedef struct fd2_counters {

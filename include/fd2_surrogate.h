@@ -3,8 +3,8 @@
  *
  * No counterpart in the reference: hybridMANTIS always runs the full
  * optical Monte Carlo.  This is a small MLP that maps one energy
- * deposition (depth below the entrance surface, deposited energy, offset in
- * its column) and the detector geometry (thickness, column radius,
+ * deposition (depth below the entrance surface, deposited energy, lateral
+ * distance from the detector centre) and the detector geometry (thickness, column radius,
  * roughness, top reflectivity, bulk absorption) to
  *   - the probability that one optical photon from it is detected, and
  *   - the radial distribution of the detected photons around the deposition
@@ -23,7 +23,10 @@
  * Feature vector (FD2_SG_FEATURES floats), in physical units:
  *   0 depth below the entrance (top) surface, um   (z = H/2 - depth)
  *   1 deposited energy, keV
- *   2 offset from the column axis, in units of the column radius
+ *   2 lateral distance of the deposition from the detector centre, in units
+ *     of 50 um (photons that reach the detector's sides are lost, so the
+ *     detected fraction falls with it: about -5e-6 per um^2 of r^2 on the
+ *     500 um detector, -0.07 % at 10 um and -1.2 % at 50 um)
  *   3 thickness H, um     4 column radius R, um    5 roughness beta
  *   6 top reflectivity (1 - top_absfrac)           7 log10(bulk absorption, 1/um)
  * Network outputs (FD2_SG_OUTPUTS per point): [0] detection logit,

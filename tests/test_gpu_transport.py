@@ -101,7 +101,8 @@ def test_results_independent_of_launch_shape(require_gpu):
     outs = []
     for kw in [dict(), dict(block_size=128, chunk=8, refill=4, prf_window=0),
                dict(block_size=256, ctas_per_sm=3, refill=8, fresnel_batch=4),
-               dict(block_size=512, ctas_per_sm=1, chunk=64, use_graph=False)]:
+               dict(block_size=512, ctas_per_sm=1, chunk=64, use_graph=False),
+               dict(tally_mode=1), dict(tally_mode=1, block_size=320, ctas_per_sm=2, prf_window=48)]:
         with _run_given(es, N, seed=77, **kw) as t:
             c = t.counters()
             c.pop("photon_distance")
