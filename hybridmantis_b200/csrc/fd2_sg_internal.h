@@ -69,6 +69,11 @@ struct fd2_sg {
     double *d_acc = nullptr;
     float *d_lr = nullptr;  // Adam step size (read by the captured step)
     float *ws = nullptr;  // split-K partials
+    int64_t ws_floats = 0;
+    // tcgen05 backward: transposed BF16 weights (W2^T, W3^T: H x H; W4^T:
+    // H x 64) and batch-major operands transposed to [columns][rows padded
+    // to 256] (tA: the incoming gradient, tB: the layer's input)
+    __nv_bfloat16 *pbT = nullptr, *tA = nullptr, *tB = nullptr;
 
     // activations for up to cap_rows rows
     int cap_rows = 0;

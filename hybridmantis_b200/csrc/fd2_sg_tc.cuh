@@ -1,9 +1,13 @@
-// fd2_sg_tc.cuh -- the surrogate's forward GEMMs on the 5th-generation tensor
-// cores: tcgen05.mma with the accumulator in tensor memory (TMEM).
+// fd2_sg_tc.cuh -- the surrogate's GEMMs on the 5th-generation tensor cores:
+// tcgen05.mma with the accumulator in tensor memory (TMEM).
 //
 // C[M x N] = A[M x K] B[N x K]^T (both operands K-contiguous, BF16), FP32
-// accumulation, epilogue bias + ReLU to BF16 or bias to FP32 -- the four
-// forward products of the MLP (kc x kc in fd2_sg_gemm.cuh).  Persistent CTAs
+// accumulation, epilogue bias + ReLU to BF16, bias to FP32, ReLU mask to
+// BF16 or plain FP32 -- the four forward products of the MLP (kc x kc in
+// fd2_sg_gemm.cuh) and, with the weights and the batch-major operands
+// transposed first, the backward products: input gradients dY W (mask
+// epilogue) and weight gradients dY^T X split over 256-row slices of the
+// batch (blockIdx.y = slice, FP32 partial planes).  Persistent CTAs
 // of four warps (at most one per SM) walk the 128-row tiles, the whole
 // contraction of a tile in one pass:
 //   1. the CTA stages all of B (N x K) once and, per tile, its A tile
@@ -50,10 +54,13 @@ struct TcArgs {
     const __nv_bfloat16 *B;
     int lda, ldb, M, N, K;
     const int *m_limit;
-    int epi;  // kEpiBiasReluBf16 or kEpiBiasF32
+    int epi;  // kEpiBiasReluBf16, kEpiBiasF32, kEpiMaskBf16 or kEpiPartialF32
     const float *bias;
+    const __nv_bfloat16 *mask;  // kEpiMaskBf16: out = acc * (mask[row][col] > 0)
+    int ldm;
     void *C;
     int ldc;
+    long long a_split, b_split, c_split;  // element offsets of slice blockIdx.y
     unsigned *fault;  // set when a wait gives up (the tile is then not stored)
 };
 
@@ -135,6 +142,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
     const int ntiles = (M + kTcRows - 1) / kTcRows;
     if ((int)blockIdx.x >= ntiles) return;  // whole CTA, before any TMEM or barrier use
     const int N = g.N, K = g.K;
+    const __nv_bfloat16 *gA = g.A + (long long)blockIdx.y * g.a_split;
+    const __nv_bfloat16 *gB = g.B + (long long)blockIdx.y * g.b_split;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char *sA = tc_smem;
     unsigned char *sB = tc_smem + (size_t)kTcRows * K * 2;
@@ -152,7 +161,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
         s_ok = 1;
     }
     // B stays resident for all of the CTA's tiles
-    tc_stage(sB, g.B, g.ldb, N, N, K);
+    tc_stage(sB, gB, g.ldb, N, N, K);
     const uint32_t idesc = tc_instr_desc(kTcRows, N);
     const uint32_t lbo_a = kTcRows * 16, lbo_b = (uint32_t)N * 16;
     uint32_t taddr = 0;
@@ -160,7 +169,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int m0 = tile * kTcRows;
         const int valid = min(kTcRows, M - m0);
-        tc_stage(sA, g.A + (long long)m0 * g.lda, g.lda, kTcRows, valid, K);
+        tc_stage(sA, gA + (long long)m0 * g.lda, g.lda, kTcRows, valid, K);
         asm volatile("cp.async.wait_all;" ::: "memory");
         // the staged operands become visible to the tensor core's (async)
         // proxy; the previous tile's TMEM reads are ordered before the MMAs
@@ -219,16 +228,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
             if (r < valid) {
                 float f[16];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) f[j] = __uint_as_float(v[j]) + g.bias[c0 + j];
-                if (kEpi == kEpiBiasReluBf16) {
+                for (int j = 0; j < 16; ++j)
+                    f[j] = __uint_as_float(v[j]) + ((kEpi == kEpiBiasReluBf16 || kEpi == kEpiBiasF32) ? g.bias[c0 + j] : 0.0f);
+                if (kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) {
                     __align__(16) __nv_bfloat16 o[16];
+                    if (kEpi == kEpiBiasReluBf16) {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(fmaxf(f[j], 0.0f));
+                        for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(fmaxf(f[j], 0.0f));
+                    } else {
+                        __align__(16) __nv_bfloat16 mk[16];
+                        const uint4 *ms = reinterpret_cast<const uint4 *>(g.mask + row * g.ldm + c0);
+                        reinterpret_cast<uint4 *>(mk)[0] = ms[0];
+                        reinterpret_cast<uint4 *>(mk)[1] = ms[1];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            o[j] = __float2bfloat16(__bfloat162float(mk[j]) > 0.0f ? f[j] : 0.0f);
+                    }
                     uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) + row * g.ldc + c0);
                     dst[0] = reinterpret_cast<const uint4 *>(o)[0];
                     dst[1] = reinterpret_cast<const uint4 *>(o)[1];
                 } else {
-                    float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(g.C) + row * g.ldc + c0);
+                    float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(g.C) + (long long)blockIdx.y * g.c_split +
+                                                             row * g.ldc + c0);
 #pragma unroll
                     for (int j = 0; j < 4; ++j) dst[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
                 }

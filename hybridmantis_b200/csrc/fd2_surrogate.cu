@@ -278,6 +278,26 @@ __global__ void to_bf16_kernel(const float *__restrict__ p, __nv_bfloat16 *__res
         pb[i] = __float2bfloat16(p[i]);
 }
 
+// out[c][r] = in[r][c] for r < rows, 0 for rows <= r < rows_pad (BF16,
+// 32 x 32 tiles through shared memory; in is [rows][ld_in], out
+// [cols][rows_pad]).  Feeds the tcgen05 backward products, whose operands
+// must be contiguous along the contraction.
+__global__ void transpose_bf16_kernel(const __nv_bfloat16 *__restrict__ in, int ld_in, int rows, int cols,
+                                      int rows_pad, __nv_bfloat16 *__restrict__ out)
+{
+    __shared__ __nv_bfloat16 t[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        t[i][threadIdx.x] = (r < rows && c < cols) ? in[(int64_t)r * ld_in + c] : __float2bfloat16(0.0f);
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (c < cols && r < rows_pad) out[(int64_t)c * rows_pad + r] = t[threadIdx.x][i];
+    }
+}
+
 // Normalised inputs of host-given feature rows.
 __global__ void input_kernel(const float *__restrict__ feat, int64_t n, NormParams norm, __nv_bfloat16 *__restrict__ x0)
 {
@@ -363,7 +383,7 @@ static cudaError_t sg_dense(fd2_sg *s, cudaStream_t st, const GemmArgs &g)
         if ((int64_t)g.M > (int64_t)65535 * kBM) return cudaErrorInvalidValue;  // one grid row per 64 rows
         return sg_gemm(st, true, true, g, 1);
     }
-    TcArgs t;
+    TcArgs t{};
     t.A = g.A;
     t.B = g.B;
     t.lda = g.lda;
@@ -438,12 +458,129 @@ cudaError_t weight_grad(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *dy, int
     return cudaGetLastError();
 }
 
+constexpr int kTcSlice = 256;  // batch rows per weight-gradient slice (the contraction of one tcgen05 pass)
+
+int rows_pad(int rows) { return (rows + kTcSlice - 1) / kTcSlice * kTcSlice; }
+
+cudaError_t launch_transpose(cudaStream_t st, const __nv_bfloat16 *in, int ld_in, int rows, int cols,
+                             __nv_bfloat16 *out)
+{
+    const int rp = rows_pad(rows);
+    transpose_bf16_kernel<<<dim3((unsigned)(rp / 32), (unsigned)((cols + 31) / 32)), dim3(32, 8), 0, st>>>(
+        in, ld_in, rows, cols, rp, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc(fd2_sg *s, cudaStream_t st, const TcArgs &t, unsigned grid_x, unsigned grid_y)
+{
+    const size_t smem = tc_smem_bytes(t.N, t.K);
+    const dim3 grid(grid_x, grid_y);
+    if (t.epi == kEpiBiasReluBf16) gemm_tc_kernel<kEpiBiasReluBf16><<<grid, kTcThreads, smem, st>>>(t);
+    else if (t.epi == kEpiBiasF32) gemm_tc_kernel<kEpiBiasF32><<<grid, kTcThreads, smem, st>>>(t);
+    else if (t.epi == kEpiMaskBf16) gemm_tc_kernel<kEpiMaskBf16><<<grid, kTcThreads, smem, st>>>(t);
+    else if (t.epi == kEpiPartialF32) gemm_tc_kernel<kEpiPartialF32><<<grid, kTcThreads, smem, st>>>(t);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+// The backward products fit one tcgen05 pass per tile when every
+// contraction (64 outputs, H hidden, 256-row batch slices) is <= 256 and
+// every width a multiple of 16.
+bool tc_backward_ok(const fd2_sg *s, int rows)
+{
+    const int H = s->hidden;
+    return s->use_tc && s->tA && H % 16 == 0 && H >= 32 && H <= kTcMaxN && rows > 0 && rows <= s->cap_rows;
+}
+
+// Weight gradient on tcgen05: dW [M][K] = sum over 256-row slices z of
+// dy_z^T x_z, with dy^T ([M][rows_pad]) and x^T ([K][rows_pad]) staged
+// contiguous along the batch; one CTA per (128-row tile of dW, slice), FP32
+// partial planes summed in slice order (deterministic).
+cudaError_t weight_grad_tc(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *dy, int ldy, int M,
+                           const __nv_bfloat16 *x, int ldx, int K, int rows, float *dw)
+{
+    cudaError_t e;
+    const int rp = rows_pad(rows), z = rp / kTcSlice;
+    if ((int64_t)z * M * K > s->ws_floats) return cudaErrorInvalidValue;
+    if ((e = launch_transpose(st, dy, ldy, rows, M, s->tA)) != cudaSuccess) return e;
+    if ((e = launch_transpose(st, x, ldx, rows, K, s->tB)) != cudaSuccess) return e;
+    TcArgs t{};
+    t.A = s->tA;
+    t.B = s->tB;
+    t.lda = rp;
+    t.ldb = rp;
+    t.M = M;
+    t.N = K;
+    t.K = kTcSlice;
+    t.epi = kEpiPartialF32;
+    t.C = s->ws;
+    t.ldc = K;
+    t.a_split = kTcSlice;
+    t.b_split = kTcSlice;
+    t.c_split = (long long)M * K;
+    t.fault = s->d_tc_fault;
+    if ((e = launch_tc(s, st, t, (unsigned)((M + kTcRows - 1) / kTcRows), (unsigned)z)) != cudaSuccess) return e;
+    split_sum_kernel<<<grid_for((int64_t)M * K, 256), 256, 0, st>>>(s->ws, z, (int64_t)M * K, dw);
+    return cudaGetLastError();
+}
+
+// Input gradient on tcgen05: d [rows][H] = (dy [rows][Nout] W [Nout][H]) *
+// (h > 0), with W^T ([H][Nout]) as the K-contiguous second operand.
+cudaError_t input_grad_tc(fd2_sg *s, cudaStream_t st, const __nv_bfloat16 *dy, int Nout, const __nv_bfloat16 *wT,
+                          const __nv_bfloat16 *h, int rows, __nv_bfloat16 *d)
+{
+    const int H = s->hidden;
+    TcArgs t{};
+    t.A = dy;
+    t.B = wT;
+    t.lda = Nout;
+    t.ldb = Nout;
+    t.M = rows;
+    t.N = H;
+    t.K = Nout;
+    t.epi = kEpiMaskBf16;
+    t.mask = h;
+    t.ldm = H;
+    t.C = d;
+    t.ldc = H;
+    t.fault = s->d_tc_fault;
+    return launch_tc(s, st, t, (unsigned)std::min((rows + kTcRows - 1) / kTcRows, s->sm_count), 1);
+}
+
 // Backward pass from dout (BF16 [rows][64], already scaled by 1/rows).
 cudaError_t backward(fd2_sg *s, cudaStream_t st, int rows)
 {
     const int H = s->hidden;
     cudaError_t e;
     float *G = s->g;
+    if (tc_backward_ok(s, rows)) {
+        // the weights' transposes (BF16 copies of this step's parameters)
+        __nv_bfloat16 *w2T = s->pbT, *w3T = s->pbT + (size_t)H * H, *w4T = s->pbT + 2 * (size_t)H * H;
+        const dim3 tb(32, 8), tg((unsigned)((H + 31) / 32), (unsigned)((H + 31) / 32));
+        transpose_bf16_kernel<<<dim3((unsigned)((kOutPad + 31) / 32), tg.y), tb, 0, st>>>(s->pb + s->off[kW4], H,
+                                                                                          kOutPad, H, kOutPad, w4T);
+        transpose_bf16_kernel<<<tg, tb, 0, st>>>(s->pb + s->off[kW3], H, H, H, H, w3T);
+        transpose_bf16_kernel<<<tg, tb, 0, st>>>(s->pb + s->off[kW2], H, H, H, H, w2T);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        // layer 4
+        if ((e = weight_grad_tc(s, st, s->dout, kOutPad, kOutPad, s->h3, H, H, rows, G + s->off[kW4])) != cudaSuccess)
+            return e;
+        colsum_kernel<<<(kOutPad + 31) / 32, 1024, 0, st>>>(s->dout, kOutPad, rows, kOutPad, G + s->off[kB4]);
+        if ((e = input_grad_tc(s, st, s->dout, kOutPad, w4T, s->h3, rows, s->d3)) != cudaSuccess) return e;
+        // layer 3
+        if ((e = weight_grad_tc(s, st, s->d3, H, H, s->h2, H, H, rows, G + s->off[kW3])) != cudaSuccess) return e;
+        colsum_kernel<<<(H + 31) / 32, 1024, 0, st>>>(s->d3, H, rows, H, G + s->off[kB3]);
+        if ((e = input_grad_tc(s, st, s->d3, H, w3T, s->h2, rows, s->d2)) != cudaSuccess) return e;
+        // layer 2
+        if ((e = weight_grad_tc(s, st, s->d2, H, H, s->h1, H, H, rows, G + s->off[kW2])) != cudaSuccess) return e;
+        colsum_kernel<<<(H + 31) / 32, 1024, 0, st>>>(s->d2, H, rows, H, G + s->off[kB2]);
+        if ((e = input_grad_tc(s, st, s->d2, H, w2T, s->h1, rows, s->d1)) != cudaSuccess) return e;
+        // layer 1
+        if ((e = weight_grad_tc(s, st, s->d1, H, H, s->x0, kInPad, kInPad, rows, G + s->off[kW1])) != cudaSuccess)
+            return e;
+        colsum_kernel<<<(H + 31) / 32, 1024, 0, st>>>(s->d1, H, rows, H, G + s->off[kB1]);
+        return cudaGetLastError();
+    }
     // layer 4
     if ((e = weight_grad(s, st, s->dout, kOutPad, kOutPad, s->h3, H, H, rows, G + s->off[kW4])) != cudaSuccess)
         return e;
@@ -592,6 +729,15 @@ fd2_status ensure_rows(fd2_sg *s, int rows)
 {
     if (rows <= s->cap_rows) return FD2_OK;
     const size_t H = (size_t)s->hidden, R = (size_t)rows;
+    // tcgen05 backward: transposed operands over the rows padded to 256, and
+    // one FP32 partial plane per 256-row slice
+    const size_t RP = (size_t)rows_pad(rows);
+    SG_CUDA(s, alloc(&s->tA, std::max<size_t>(H, kOutPad) * RP));
+    SG_CUDA(s, alloc(&s->tB, std::max<size_t>(H, kInPad) * RP));
+    const size_t plane = std::max<size_t>(H * H, (size_t)kOutPad * H);
+    const size_t wsf = std::max<size_t>((size_t)kMaxSplits, RP / kTcSlice) * plane;
+    SG_CUDA(s, alloc(&s->ws, wsf));
+    s->ws_floats = (int64_t)wsf;
     SG_CUDA(s, alloc(&s->x0, R * kInPad));
     SG_CUDA(s, alloc(&s->h1, R * H));
     SG_CUDA(s, alloc(&s->h2, R * H));
@@ -678,7 +824,7 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     const size_t P = (size_t)s->n_params;
     if (alloc(&s->p, P) || alloc(&s->g, P) || alloc(&s->m, P) || alloc(&s->v, P) || alloc(&s->pb, P) ||
         alloc(&s->d_live, P) || alloc(&s->d_step, 1) || alloc(&s->d_acc, 4) || alloc(&s->d_lr, 1) ||
-        alloc(&s->ws, (size_t)kMaxSplits * std::max<size_t>((size_t)s->hidden * s->hidden, (size_t)kOutPad * s->hidden)))
+        alloc(&s->pbT, 2 * (size_t)s->hidden * s->hidden + (size_t)s->hidden * kOutPad))
         return bail(FD2_ERR_OUT_OF_MEMORY);
     if (cudaMemcpy(s->d_lr, &s->lr, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return bail(FD2_ERR_CUDA);
     if (alloc(&s->d_tc_fault, 1) || cudaMemset(s->d_tc_fault, 0, sizeof(unsigned)) != cudaSuccess)
@@ -694,6 +840,10 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
         if (cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasReluBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
                 cudaSuccess ||
             cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(gemm_tc_kernel<kEpiMaskBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(gemm_tc_kernel<kEpiPartialF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
                 cudaSuccess)
             return bail(FD2_ERR_CUDA);
     }
@@ -745,7 +895,8 @@ void fd2_sg_destroy(fd2_sg *s)
                     (void *)s->d_step, (void *)s->d_acc, (void *)s->d_lr, (void *)s->ws, (void *)s->x0, (void *)s->h1, (void *)s->h2,
                     (void *)s->h3, (void *)s->d1, (void *)s->d2, (void *)s->d3, (void *)s->out, (void *)s->dout,
                     (void *)s->target, (void *)s->has_rad, (void *)s->ylab, (void *)s->d_feat, (void *)s->d_photons,
-                    (void *)s->d_detected, (void *)s->d_radial, (void *)s->d_tc_fault})
+                    (void *)s->d_detected, (void *)s->d_radial, (void *)s->d_tc_fault, (void *)s->pbT, (void *)s->tA,
+                    (void *)s->tB})
         if (p) cudaFree(p);
     sg_free_run_buffers(s);
     if (s->stream) cudaStreamDestroy(s->stream);

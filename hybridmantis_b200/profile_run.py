@@ -25,12 +25,14 @@ def main():
     ap.add_argument("--fresnel", type=int, default=0)
     ap.add_argument("--grid", type=int, default=0, help="1 / 2: explicit square / hexagonal column lattice")
     ap.add_argument("--gap", type=float, default=0.5, help="lattice gap between columns (um)")
+    ap.add_argument("--tally-mode", type=int, default=0,
+                    help="0: per-lane L2 reductions; 1: warp-aggregated, shared-memory privatised tallies")
     a = ap.parse_args()
     es = fd.synth_events(a.config, a.xrays, a.seed)
     x, y, z = es.to_cm()
     with fd.OpticalTransport(es.params, block_size=a.block, ctas_per_sm=a.ctas, chunk=a.chunk, refill=a.refill,
                              prf_window=a.window, fresnel_batch=a.fresnel, column_grid=a.grid,
-                             grid_gap_um=a.gap) as t:
+                             grid_gap_um=a.gap, tally_mode=a.tally_mode) as t:
         t.submit_events(x, y, z, es.e_ev.astype(np.float64), es.hist)
         out = []
         for _ in range(a.runs):

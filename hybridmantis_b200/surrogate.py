@@ -71,10 +71,12 @@ def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: i
     """Monte Carlo labels: for each geometry, `points_per_geom` depositions
     with depth H u (half of them) or H u^2 (the other half: denser near the
     entrance surface, where x-rays deposit most and the PRF is widest),
-    u ~ U(0, 1), energy U(energy_kev), placed uniformly over the disc of
-    radius `lateral_um` around the detector centre (the detected fraction
-    falls with the distance from the centre, as photons reach the detector's
-    sides), each transported with `photons` photons.  Returns
+    u ~ U(0, 1), energy U(energy_kev), at a distance r from the detector
+    centre (uniform azimuth) with r = lateral_um sqrt(v) for half of them
+    (uniform over the disc) and lateral_um v^2 for the other half (dense near
+    the centre, where the events of a pencil beam lie), v ~ U(0, 1) -- the
+    detected fraction falls with r as photons reach the detector's sides --
+    each transported with `photons` photons.  Returns
     (features [n, 8], photons [n], detected [n], radial [n, radial_bins + 1])."""
     rng = np.random.default_rng(seed)
     feats, phot, det, rad = [], [], [], []
@@ -90,7 +92,11 @@ def label_points(geoms, points_per_geom: int, photons: int, seed: int, device: i
             u = rng.uniform(0.001, 0.999, n)
             u = np.where(rng.random(n) < 0.5, u, np.maximum(u * u, 0.001))
             depth = (H * u).astype(np.float32).astype(np.float64)
-            lat = lateral_um * np.sqrt(rng.uniform(0.0, 1.0, n))
+            # half uniform over the disc, half with density ~ r^-1/2 (r = R u^2):
+            # in-loop events sit mostly within ~10 um of the beam, where a
+            # uniform disc would put few labels
+            ul = rng.uniform(0.0, 1.0, n)
+            lat = lateral_um * np.where(rng.random(n) < 0.5, np.sqrt(ul), ul * ul)
             phi = rng.uniform(0.0, 2.0 * np.pi, n)
             cx = (np.array([g.det_x / 2.0 for g in gs])[gi] + lat * np.cos(phi)).astype(np.float32)
             cy = (np.array([g.det_y / 2.0 for g in gs])[gi] + lat * np.sin(phi)).astype(np.float32)

@@ -41,6 +41,8 @@ def main():
     ap.add_argument("--lr-min", type=float, default=1e-5)
     ap.add_argument("--init", default="")
     ap.add_argument("--focus", type=int, default=-1)
+    ap.add_argument("--radial-weight", type=float, default=1.0,
+                    help="weight of the radial cross-entropy against the detection BCE in the loss")
     ap.add_argument("--out", default="")
     a = ap.parse_args()
     t0 = time.perf_counter()
@@ -55,7 +57,7 @@ def main():
     perm = np.random.default_rng(a.seed + 2).permutation(len(f))
     f, ph, det, rad = f[perm], ph[perm], det[perm], rad[perm]
     n_val = int(a.val * len(f))
-    with sgm.Surrogate(device=a.device, batch=a.batch, lr=a.lr, seed=a.seed + 3) as s:
+    with sgm.Surrogate(device=a.device, batch=a.batch, lr=a.lr, seed=a.seed + 3, radial_weight=a.radial_weight) as s:
         if a.init:
             s.load(a.init)
         s.set_data(f, ph, det, rad, n_val=n_val)

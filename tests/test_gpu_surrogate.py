@@ -64,7 +64,9 @@ def test_gradients_match_oracle(require_gpu):
 
 def test_label_mode_counts_every_detected_photon(require_gpu):
     geoms = sgm.sample_geometries(3, seed=5)
-    f, ph, det, rad = sgm.label_points(geoms, 40, 1500, seed=9)
+    # depositions at the detector centre (lateral_um=0), so the comparison run
+    # below can place the same photons
+    f, ph, det, rad = sgm.label_points(geoms, 40, 1500, seed=9, lateral_um=0.0)
     assert f.shape == (120, 8) and rad.shape == (120, 97)
     assert np.array_equal(det, rad.sum(1).astype(np.int32))
     assert np.all(det <= ph) and 0.02 < det.sum() / ph.sum() < 0.98
@@ -161,3 +163,36 @@ def test_tensor_core_forward_matches_mma_sync(require_gpu, monkeypatch):
     # activation by one BF16 step now and then
     assert np.abs(a - b).max() <= 2e-2 * scale, np.abs(a - b).max()
     assert np.abs(a - b).mean() <= 1e-3 * scale, np.abs(a - b).mean()
+
+
+def test_tensor_core_backward_matches_mma_sync(require_gpu, monkeypatch):
+    """The backward products run on tcgen05 too: input gradients dY W with
+    the weights transposed once per step, weight gradients dY^T X over
+    256-row slices of the batch with both operands transposed to be
+    contiguous along the batch (FP32 partial planes summed in slice order).
+    Against the mma.sync kernels (FD2_SG_GEMM=mma) on a full-size network and
+    a ragged batch of 3,000 rows (12 slices, the last one partly padding):
+    every parameter block's gradient agrees to BF16 accuracy."""
+    H, n = 256, 3000
+    p, f, lo, hi, ph, de, ra = _random_problem(17, n, H)
+    grads = []
+    for mode in ("tc", "mma"):
+        if mode == "mma":
+            monkeypatch.setenv("FD2_SG_GEMM", "mma")
+        else:
+            monkeypatch.delenv("FD2_SG_GEMM", raising=False)
+        with sgm.Surrogate(hidden=H, batch=4096, radial_bins=64, radial_max_um=200.0) as s:
+            s.set_params(p)
+            s.set_hull(lo, hi)
+            loss, g = s.loss_grad(f, ph, de, ra)
+            grads.append((loss, g.astype(np.float64)))
+    (la, ga), (lb, gb) = grads
+    assert abs(la - lb) <= 1e-5 * abs(lb)
+    sizes = [H * 8, H, H * H, H, H * H, H, 25 * H, 25]
+    o = 0
+    for name, k in zip(BLOCKS, sizes):
+        a, b = ga[o:o + k], gb[o:o + k]
+        o += k
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        cos = a @ b / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-30)
+        assert np.all(np.isfinite(a)) and rel < 1e-2 and cos > 0.9999, (name, rel, cos)
