@@ -219,7 +219,8 @@ void choose_window_sums(fd2_ctx *c, double sx, double sy, int64_t k)
     int w = c->opt.prf_window;
     if (w < 0) w = 128;
     if (c->d_radial) w = 0;  // label mode tallies no PRF image
-    if (c->opt.tally_mode == 0) w = 0;  // per-lane reductions go straight to the global PRF
+    if (!(c->opt.tally_mode == 1 && c->geoms.size() == 1 && !c->opt.column_grid))
+        w = 0;  // per-lane reductions go straight to the global PRF
     if (w > g.xdim) w = g.xdim;
     if (w > g.ydim) w = g.ydim;
     if (w > 176) w = 176;  // fits beside the rings in shared memory
@@ -275,7 +276,6 @@ fd2::TransportArgs transport_args(fd2_ctx *c)
     a.refill = c->cfg.refill;
     a.fresnel_batch = c->cfg.fresnel;
     a.window = c->cfg.window;
-    a.tally_direct = c->opt.tally_mode == 0 ? 1 : 0;
     a.win_x0 = c->win_x0;
     a.win_y0 = c->win_y0;
     a.abort_flag = c->d_abort;
@@ -404,6 +404,9 @@ fd2_status set_config(fd2_ctx *c, const fd2::TransportConfig &cfg)
     k.chunk = std::min(std::max(k.chunk, 1), 4096);
     k.refill = std::min(std::max(k.refill, 1), 32);
     k.fresnel = std::min(std::max(k.fresnel, 1), 32);
+    // warp-aggregated, shared-memory privatised tallies: single-geometry runs
+    // of the reference's column model (the other kernels reduce per lane)
+    k.aggregate = c->opt.tally_mode == 1 && c->geoms.size() == 1 && !c->opt.radial_bins && !c->opt.column_grid;
     c->cfg = k;
     fit_window(c);
     FD2_CUDA(c, fd2::prepare_transport(c->cfg, (int)c->geoms.size()));

@@ -17,6 +17,7 @@ struct TransportConfig {
     int refill = 1;      // idle lanes that trigger a warp refill
     int window = 0;      // shared-memory PRF window edge (0 = off)
     int fresnel = 8;     // parked lanes that trigger the warp's Fresnel pass
+    bool aggregate = false;  // single geometry: warp-aggregated, shared-memory privatised tallies
 };
 
 struct TransportArgs {
@@ -43,7 +44,6 @@ struct TransportArgs {
     int refill;
     int fresnel_batch;           // parked lanes before the Fresnel pass runs
     int window;                  // window edge (0 = off), applies to geometry 0
-    int tally_direct;            // 1: per-lane global reductions; 0: warp-aggregated, shared-memory privatised
     int win_x0, win_y0;          // window origin in pixels
     const volatile int *abort_flag;
     int *status;

@@ -332,14 +332,14 @@ struct SmemLayout {
 // refill > 1, once enough lanes of the warp are) idle, so lanes never wait
 // for the longest walk in the warp.  Tallies: by default every ended photon
 // adds to the global fates, per-primary counts and PRF with one L2
-// reduction of its lane; with tally_direct = 0 they are aggregated across
+// reduction of its lane; with kAgg (tally_mode 1) they are aggregated across
 // the warp before touching memory and the PRF core of geometry 0 is tallied
 // in a shared-memory window (identical tallies, slower on a B200).  kMulti: the
 // geometry of each photon comes from the table in shared memory; otherwise
 // the single geometry is read from the kernel parameters.  kRadial (label
 // mode): a detected photon is binned by its distance from its event into
 // the history's radial histogram instead of the PRF image.
-template <bool kMulti, int kMaxThreads, int kMinBlocks, bool kRadial = false, bool kGrid = false>
+template <bool kMulti, int kMaxThreads, int kMinBlocks, bool kRadial = false, bool kGrid = false, bool kAgg = false>
 __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(const __grid_constant__ TransportArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -504,13 +504,13 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
         }
 
         // ---- tallies of the photons that ended: one global reduction per lane
-        // (tally_direct), or aggregated across the warp and privatised in
+        // (the default), or (kAgg) aggregated across the warp and privatised in
         // shared memory
         const unsigned ended = __ballot_sync(kFull, fate != kAlive);
         if (ended) {
             if (fate != kAlive) {
                 const unsigned key = (unsigned)(geom * kCounterStride + fate);
-                if (a.tally_direct) {
+                if (!kAgg) {
                     atomicAdd(&a.counters[key], 1ull);
                 } else {
                     const unsigned peers = __match_any_sync(ended, key);
@@ -524,7 +524,7 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
             if (fate == kDetect) {
                 const float4 ev = s_lane[threadIdx.x];
                 const int prim = __float_as_int(ev.w);
-                if (a.tally_direct) {
+                if (!kAgg) {
                     if ((unsigned)prim < (unsigned)a.n_prim) atomicAdd(&a.per_primary[prim], 1);
                 } else {
                     const unsigned peers = __match_any_sync(det, prim);
@@ -542,10 +542,10 @@ __global__ void __launch_bounds__(kMaxThreads, kMinBlocks) transport_kernel(cons
                     if ((unsigned)prim < (unsigned)a.n_prim && b >= 0)
                         atomicAdd(&a.radial[(long long)prim * (a.radial_bins + 1) + b], 1u);
                 } else if (w.ii >= 0 && w.jj >= 0 && w.ii < xdim && w.jj < ydim) {
-                    if (a.tally_direct) atomicAdd(&a.counters[geom * kCounterStride + kNumFates], 1ull);
+                    if (!kAgg) atomicAdd(&a.counters[geom * kCounterStride + kNumFates], 1ull);
                     else atomicAdd(&s_cnt[geom * kCounterStride + kNumFates], 1u);
                     const int wx = w.ii - a.win_x0, wy = w.jj - a.win_y0;
-                    if (geom == 0 && win > 0 && (unsigned)wx < (unsigned)win && (unsigned)wy < (unsigned)win) {
+                    if (kAgg && geom == 0 && win > 0 && (unsigned)wx < (unsigned)win && (unsigned)wy < (unsigned)win) {
                         atomicAdd(&s_win[wx * win + wy], 1u);
                     } else {
                         const long long off = kMulti ? s_geom[geom].prf_offset : a.g0.prf_offset;
@@ -714,14 +714,17 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
 // resident CTAs per SM (128, 85, 64 registers), blocks of 320 threads for
 // two (102 registers: 20 warps per SM; the walk fits without spills, 352
 // threads would spill), other larger blocks for one.
-#define FD2_TRANSPORT_VARIANTS(X)                                        \
-    X(false, 512, 1, false, false) X(false, 256, 2, false, false)        \
-    X(false, 320, 2, false, false) X(true, 320, 2, false, false)         \
-    X(false, 256, 2, false, true) X(false, 320, 2, false, true)          \
-    X(false, 256, 3, false, false) X(false, 256, 4, false, false)        \
-    X(true, 512, 1, false, false) X(true, 256, 2, false, false)          \
-    X(true, 256, 3, false, false) X(true, 256, 2, true, false)          \
-    X(true, 256, 4, false, false) X(false, 256, 3, false, true)
+#define FD2_TRANSPORT_VARIANTS(X)                                                          \
+    X(false, 512, 1, false, false, false) X(false, 256, 2, false, false, false)            \
+    X(false, 320, 2, false, false, false) X(true, 320, 2, false, false, false)             \
+    X(false, 256, 2, false, true, false) X(false, 320, 2, false, true, false)              \
+    X(false, 256, 3, false, false, false) X(false, 256, 4, false, false, false)            \
+    X(true, 512, 1, false, false, false) X(true, 256, 2, false, false, false)              \
+    X(true, 256, 3, false, false, false) X(true, 256, 2, true, false, false)               \
+    X(true, 256, 4, false, false, false) X(false, 256, 3, false, true, false)              \
+    X(false, 512, 1, false, false, true) X(false, 256, 2, false, false, true)              \
+    X(false, 320, 2, false, false, true) X(false, 256, 3, false, false, true)              \
+    X(false, 256, 4, false, false, true)
 
 cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
 {
@@ -735,14 +738,14 @@ cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
     if (e != cudaSuccess) return e;
     const size_t need = transport_smem_bytes(cfg, n_geom);
     // dynamic limit = opt-in maximum - the kernel's static shared memory
-#define FD2_SET_ATTR(M, T, B, R, L)                                                                       \
+#define FD2_SET_ATTR(M, T, B, R, L, A)                                                                       \
     if (e == cudaSuccess) {                                                                               \
         cudaFuncAttributes fa;                                                                            \
-        e = cudaFuncGetAttributes(&fa, transport_kernel<M, T, B, R, L>);                                  \
+        e = cudaFuncGetAttributes(&fa, transport_kernel<M, T, B, R, L, A>);                                  \
         const int lim = max_optin - (int)fa.sharedSizeBytes;                                              \
         if (e == cudaSuccess && need > (size_t)lim) e = cudaErrorInvalidValue;                            \
         if (e == cudaSuccess)                                                                             \
-            e = cudaFuncSetAttribute(transport_kernel<M, T, B, R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim); \
+            e = cudaFuncSetAttribute(transport_kernel<M, T, B, R, L, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim); \
     }
     FD2_TRANSPORT_VARIANTS(FD2_SET_ATTR)
 #undef FD2_SET_ATTR
@@ -771,6 +774,13 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
         // label mode: one variant, 256 threads, two CTAs per SM
         if (cfg.block > 256) return cudaErrorInvalidConfiguration;
         transport_kernel<true, 256, 2, true><<<(unsigned)(sm_count * 2), cfg.block, smem, s>>>(a);
+    } else if (!multi && cfg.aggregate) {
+        // warp-aggregated, shared-memory privatised tallies (tally_mode 1)
+        if (cfg.block == 320) transport_kernel<false, 320, 2, false, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 1) transport_kernel<false, 512, 1, false, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 2) transport_kernel<false, 256, 2, false, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else if (per_sm == 3) transport_kernel<false, 256, 3, false, false, true><<<grid, cfg.block, smem, s>>>(a);
+        else transport_kernel<false, 256, 4, false, false, true><<<grid, cfg.block, smem, s>>>(a);
     } else if (!multi) {
         if (cfg.block == 320) transport_kernel<false, 320, 2><<<grid, cfg.block, smem, s>>>(a);
         else if (per_sm == 1) transport_kernel<false, 512, 1><<<grid, cfg.block, smem, s>>>(a);

@@ -221,7 +221,6 @@ extern "C" fd2_status fd2_transport_noalloc(const fd2_geometry *geometry, const 
         a.refill = cfg.refill;
         a.fresnel_batch = cfg.fresnel;
         a.window = 0;
-        a.tally_direct = 1;
         a.abort_flag = nullptr;
         a.status = flags;
         e = fd2::launch_transport(s, cfg, sms, a);

@@ -21,7 +21,26 @@ def main():
     ap.add_argument("--rows", type=int, default=65536)
     ap.add_argument("--runs", type=int, default=6)
     ap.add_argument("--hidden", type=int, default=256)
+    ap.add_argument("--train", type=int, default=0,
+                    help="instead of forward passes: this many training steps (forward, loss, the backward "
+                         "GEMMs, Adam) on --rows random labelled points, batch 8192")
     a = ap.parse_args()
+    if a.train:
+        rng = np.random.default_rng(2)
+        n = a.rows
+        f = rng.uniform(0, 1, (n, 8)).astype(np.float32)
+        ph = rng.integers(500, 3000, n).astype(np.int32)
+        det = (ph * rng.uniform(0.1, 0.6, n)).astype(np.int32)
+        rad = rng.integers(0, 40, (n, 97)).astype(np.uint32)
+        with sgm.Surrogate(hidden=a.hidden, batch=8192) as s:
+            s.set_data(f, ph, det, rad, n_val=0)
+            ms = []
+            for _ in range(a.runs):
+                t0 = time.perf_counter()
+                tl, _ = s.train(a.train)
+                ms.append((time.perf_counter() - t0) * 1e3 / a.train)
+        print(json.dumps({"gemm": os.environ.get("FD2_SG_GEMM", "tc"), "train_step_ms": ms, "loss": tl}))
+        return
     rng = np.random.default_rng(1)
     with sgm.Surrogate(hidden=a.hidden, batch=a.rows) as s:
         s.set_params(rng.normal(0, 0.05, s.num_params()).astype(np.float32))

@@ -148,10 +148,12 @@ typedef struct fd2_options {
     double grid_gap_um;            /* lattice: gap between neighbouring columns */
     int32_t tally_mode;            /* 0 (default): each ended photon adds to the
                                       global tallies with one L2 reduction of its
-                                      lane; 1: fates and per-history counts are
-                                      aggregated across the warp (__match_any_sync)
-                                      and privatised in shared memory, the PRF core
-                                      in a shared-memory window (prf_window).  The
+                                      lane; 1 (single-geometry runs of the
+                                      reference's column model): fates and
+                                      per-history counts are aggregated across the
+                                      warp (__match_any_sync) and privatised in
+                                      shared memory, the PRF core in a
+                                      shared-memory window (prf_window).  The
                                       tallies are identical; 0 is faster on a B200
                                       (the tally rate is far below the L2's atomic
                                       throughput, so aggregation only costs issue) */
