@@ -34,6 +34,17 @@ def _radial(img, cx, cy, edges):
     return h / max(h.sum(), 1.0)
 
 
+def _l1_by_radius(a, b, cx, cy, bands):
+    """Contributions to the L1 distance of two normalised images from pixels
+    in radial bands around (cx, cy) (pixel centres)."""
+    a = np.asarray(a, np.float64) / max(np.sum(a), 1.0)
+    b = np.asarray(b, np.float64) / max(np.sum(b), 1.0)
+    ii, jj = np.meshgrid(np.arange(a.shape[0]) + 0.5, np.arange(a.shape[1]) + 0.5, indexing="ij")
+    r = np.hypot(ii - cx, jj - cy)
+    d = np.abs(a - b)
+    return [float(d[(r >= lo) & (r < hi)].sum()) for lo, hi in zip(bands[:-1], bands[1:])]
+
+
 def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 4242, audit: float = 0.01,
              device: int = 0, repeats: int = 2, noise_floor: bool = False, frontend: bool = False,
              lateral_um: float = 50.0) -> dict:
@@ -109,6 +120,8 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
         "radial_prf_l1": float(np.abs(rm - rs).sum()),
         "radial_profile": {"edges_um": edges.tolist(), "mc": rm.tolist(), "sg": rs.tolist()},
         "prf_image_l1": float(np.abs(im / im.sum() - isg / isg.sum()).sum()),
+        "prf_image_l1_by_radius": {"bands_um": [0, 3, 6, 10, 20, 50, 100, 1000],
+                                   "sg_vs_mc": _l1_by_radius(isg, im, cx, cy, [0, 3, 6, 10, 20, 50, 100, 1000])},
         "detected": [res["mc"]["detected"], res["sg"]["detected"]],
         "sg_stats": res["sg"]["stats"],
     })
@@ -119,6 +132,7 @@ def evaluate(model: str, config: int = 4, xrays: int = 1_000_000, seed: int = 42
         r2 = _radial(i2, cx, cy, edges)
         out["mc_vs_mc"] = {"radial_prf_l1": float(np.abs(rm - r2).sum()),
                            "prf_image_l1": float(np.abs(im / im.sum() - i2 / i2.sum()).sum()),
+                           "prf_image_l1_by_radius": _l1_by_radius(i2, im, cx, cy, [0, 3, 6, 10, 20, 50, 100, 1000]),
                            "phs_mean": res["mc2"]["phs_mean"], "swank": res["mc2"]["swank"]}
     return out
 
