@@ -276,19 +276,22 @@ def parity_vs_reference(es, nphot, nev, ref_tallies, device, seed):
 
 
 # DRAM bytes per photon of the transport kernel: dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture (3,338,240 B for 4,690,971 photons
-# of the config-1 stream, 2,000 x-rays); the traffic is one event record per
-# chunk and grows in proportion to the photons.
-TRANSPORT_DRAM_BYTES_PER_PHOTON = 3338240.0 / 4690971.0
+# dram__bytes_write.sum of one ncu capture (26,748,000 B for 46,784,158
+# photons of the config-1 stream, 20,000 x-rays, steady state); the traffic is
+# one event record per chunk and grows in proportion to the photons.
+TRANSPORT_DRAM_BYTES_PER_PHOTON = 0.57
 # ncu counters of the transport kernel in steady state (one capture of this
 # build on 20,000 config-1 x-rays, where the launch's tail is small): issue
 # slots used (smsp__issue_active), FP32 FMA pipe busy (sm__pipe_fma_cycles_
 # active), active lanes per warp instruction (smsp__thread_inst_executed_per_
-# inst_executed) and warp instructions per photon (smsp__inst_executed.sum /
-# photons).
-TRANSPORT_NCU = {"issue_slot_utilisation": 0.554, "fp32_pipe_utilisation": 0.232,
-                 "lanes_per_instruction": 16.43, "warp_instructions_per_photon": 1628.0,
-                 "source": "ncu --clock-control none on 20,000 config-1 x-rays (transport_kernel<false,320,2>)"}
+# inst_executed), warp instructions per photon (smsp__inst_executed.sum /
+# photons) and the tallies' L2 reductions against their peak
+# (lts__t_sectors_op_red.avg.pct_of_peak_sustained_elapsed).
+TRANSPORT_NCU = {"issue_slot_utilisation": 0.734, "fp32_pipe_utilisation": 0.282,
+                 "lanes_per_instruction": 16.27, "warp_instructions_per_photon": 1198.5,
+                 "l2_reduction_pct_of_peak": 0.58,
+                 "source": "ncu --clock-control none on 20,000 config-1 x-rays "
+                           "(transport_kernel<false,256,4,false,false,false>, default launch)"}
 
 
 def bench_config(es, world):
@@ -572,7 +575,7 @@ def run_ours(a, rank, world, local_rank):
         roofline = {"bound": "fp32-issue", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                     "frac": achieved / peak_tflops,
                     "traffic": TRANSPORT_DRAM_BYTES_PER_PHOTON * photons_per_launch,
-                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 2,000-x-ray capture, "
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 20,000-x-ray capture, "
                                       "scaled by photons",
                     "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 (FMA) x {sm_max:.0f} MHz "
                                    f"(sm_max_mhz of MEASURED_PEAKS.json; the file has no FP32 entry)",
