@@ -94,6 +94,7 @@ struct fd2_sg {
     // forward GEMMs on tcgen05 (fd2_sg_tc.cuh) unless FD2_SG_GEMM=mma; a
     // tile whose completion wait gave up sets the fault word
     bool use_tc = true;
+    bool tc_pipe = true;  // the pipelined tcgen05 kernel (FD2_SG_GEMM=tc1: the one-tile-at-a-time kernel)
     unsigned *d_tc_fault = nullptr;
     int sm_count = 148;
 };

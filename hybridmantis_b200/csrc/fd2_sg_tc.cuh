@@ -261,5 +261,280 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols));
 }
 
+
+// ---------------------------------------------------------------------------
+// Pipelined variant: the same products with the stages of consecutive tiles
+// overlapped.  Six warps with fixed roles:
+//   warp 4 (producer): stages A in 128-row x 64-K chunks (16 KB) into a ring
+//     of four shared-memory stages with cp.async, then fence.proxy.async and
+//     an arrive on the stage's `full` barrier; it waits on the stage's
+//     `empty` barrier (the MMAs that read it have completed) before reuse;
+//   warp 5 (one elected thread): issues the tcgen05.mma of each chunk as soon
+//     as its stage is full, commits each stage to its `empty` barrier and each
+//     finished tile to its accumulator's `accf` barrier; two TMEM
+//     accumulators alternate between tiles, and a tile starts only when the
+//     epilogue has released its accumulator (`acce`);
+//   warps 0-3 (epilogue): drain their 32 TMEM lanes of a finished accumulator
+//     (tcgen05.ld), apply the epilogue, store, release the accumulator.
+// So the loads of the next chunks and the epilogue of the previous tile run
+// while the tensor core works.  B stays resident as before.  Every wait is
+// bounded (tc_wait); a role that gives up sets the fault word and leaves its
+// loop, the others' waits then run out too, and before the columns are
+// freed the MMA thread waits (bounded) for everything it issued.  The
+// MMAs are the simple kernel's, in the same order, so the results are
+// bitwise identical to it.
+constexpr int kPipeStages = 4;
+constexpr int kPipeThreads = 192;
+constexpr int kPipeChunkK = 64;
+
+__host__ __device__ inline int tc_pipe_chunk(int K) { return K < kPipeChunkK ? K : kPipeChunkK; }
+
+// Dynamic shared memory of one CTA: B + the A ring.
+__host__ __device__ inline size_t tc_pipe_smem_bytes(int N, int K)
+{
+    return (size_t)N * (size_t)K * sizeof(__nv_bfloat16) +
+           (size_t)kPipeStages * kTcRows * (size_t)tc_pipe_chunk(K) * sizeof(__nv_bfloat16);
+}
+
+// tc_stage for thread `tid` of `nthr` (a subset of the CTA).
+__device__ __forceinline__ void tc_stage_part(unsigned char *dst, const __nv_bfloat16 *src, int ld, int rows,
+                                              int valid, int K, int tid, int nthr)
+{
+    const int kc = K / 8;
+    const int total = rows * kc;
+    for (int L = tid; L < total; L += nthr) {
+        const int ri = L & 7, t = L >> 3;
+        const int c = t % kc, rg = t / kc;
+        const int r = rg * 8 + ri;
+        const bool ok = r < valid;
+        const __nv_bfloat16 *g = src + (long long)(ok ? r : 0) * ld + c * 8;
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + (size_t)c * rows * 16 + (size_t)rg * 128 +
+                                                               (size_t)ri * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(g), "r"(ok ? 16 : 0) : "memory");
+    }
+}
+
+__device__ __forceinline__ void tc_mbar_init(uint32_t bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void tc_mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+template <int kEpi>
+__global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcArgs g)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long s_full[kPipeStages], s_empty[kPipeStages], s_accf[2], s_acce[2],
+        s_drain;
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_fault;
+
+    int M = g.M;
+    if (g.m_limit) M = min(M, *g.m_limit);
+    const int ntiles = (M + kTcRows - 1) / kTcRows;
+    if ((int)blockIdx.x >= ntiles) return;  // whole CTA, before any TMEM or barrier use
+    const int N = g.N, K = g.K;
+    const int CK = tc_pipe_chunk(K), nck = K / CK;
+    const __nv_bfloat16 *gA = g.A + (long long)blockIdx.y * g.a_split;
+    const __nv_bfloat16 *gB = g.B + (long long)blockIdx.y * g.b_split;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *sB = tc_smem;
+    unsigned char *sRing = tc_smem + (size_t)N * K * 2;
+    const uint32_t stage_bytes = (uint32_t)(kTcRows * CK * 2);
+    const uint32_t acc_cols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
+    const uint32_t cols = 2u * acc_cols;
+
+    if (warp == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_taddr);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    const uint32_t full0 = (uint32_t)__cvta_generic_to_shared(&s_full[0]);
+    const uint32_t empty0 = (uint32_t)__cvta_generic_to_shared(&s_empty[0]);
+    const uint32_t accf0 = (uint32_t)__cvta_generic_to_shared(&s_accf[0]);
+    const uint32_t acce0 = (uint32_t)__cvta_generic_to_shared(&s_acce[0]);
+    const uint32_t drain = (uint32_t)__cvta_generic_to_shared(&s_drain);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kPipeStages; ++i) {
+            tc_mbar_init(full0 + 8u * i, 32);  // the producer warp's lanes
+            tc_mbar_init(empty0 + 8u * i, 1);  // one tcgen05.commit
+        }
+        for (int i = 0; i < 2; ++i) {
+            tc_mbar_init(accf0 + 8u * i, 1);   // one tcgen05.commit
+            tc_mbar_init(acce0 + 8u * i, 4);   // one arrive per epilogue warp
+        }
+        tc_mbar_init(drain, 1);
+        s_fault = 0;
+    }
+    // B stays resident for all of the CTA's tiles
+    tc_stage_part(sB, gB, g.ldb, N, N, K, threadIdx.x, blockDim.x);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = s_taddr;
+
+    if (warp == 4) {
+        // ---- producer
+        int gc = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+            const int m0 = tile * kTcRows;
+            const int valid = min(kTcRows, M - m0);
+            for (int c = 0; c < nck; ++c, ++gc) {
+                const int st = gc % kPipeStages;
+                const uint32_t ph = (uint32_t)((gc / kPipeStages) & 1);
+                // the warp's lanes agree on the outcome of the (bounded) wait
+                ok = __all_sync(0xFFFFFFFFu, tc_wait(empty0 + 8u * st, ph ^ 1u));
+                if (!ok) {
+                    if (lane == 0) {
+                        s_fault = 1;
+                        if (g.fault) atomicOr(g.fault, 1u);
+                    }
+                    break;
+                }
+                tc_stage_part(sRing + (size_t)st * stage_bytes, gA + (long long)m0 * g.lda + c * CK, g.lda, kTcRows,
+                              valid, CK, lane, 32);
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                tc_mbar_arrive(full0 + 8u * st);
+            }
+        }
+    } else if (warp == 5) {
+        // ---- MMA issue (one thread)
+        if (lane == 0) {
+            const uint32_t idesc = tc_instr_desc(kTcRows, N);
+            const uint32_t lbo_a = kTcRows * 16, lbo_b = (uint32_t)N * 16;
+            const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
+            const uint32_t r0 = (uint32_t)__cvta_generic_to_shared(sRing);
+            int gc = 0, it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++it) {
+                const int a = it & 1;
+                if (!tc_wait(acce0 + 8u * a, (uint32_t)((it >> 1) & 1) ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = taddr + (uint32_t)a * acc_cols;
+                for (int c = 0; c < nck; ++c, ++gc) {
+                    const int st = gc % kPipeStages;
+                    if (!tc_wait(full0 + 8u * st, (uint32_t)((gc / kPipeStages) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t a0 = r0 + (uint32_t)st * stage_bytes;
+                    for (int kk = 0; kk < CK / 16; ++kk) {
+                        const uint64_t da = tc_smem_desc(a0 + 2u * kk * lbo_a, lbo_a, 128);
+                        const uint64_t db = tc_smem_desc(b0 + (uint32_t)(c * (CK / 8) + 2 * kk) * lbo_b, lbo_b, 128);
+                        const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                            :
+                            : "r"(d), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                    tc_commit(empty0 + 8u * st);  // the stage is free once these MMAs have read it
+                }
+                if (!ok) break;
+                tc_commit(accf0 + 8u * a);  // the tile's accumulator is complete
+            }
+            if (!ok) {
+                s_fault = 1;
+                if (g.fault) atomicOr(g.fault, 1u);
+            }
+            // everything issued has completed before the columns can be freed
+            tc_commit(drain);
+            if (!tc_wait(drain, 0u)) {
+                s_fault = 1;
+                if (g.fault) atomicOr(g.fault, 1u);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp w drains TMEM lanes (tile rows) 32w .. 32w + 31
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+            const int a = it & 1;
+            // the warp's lanes agree on the outcome (tcgen05.ld below is warp-wide)
+            if (!__all_sync(0xFFFFFFFFu, tc_wait(accf0 + 8u * a, (uint32_t)((it >> 1) & 1)))) {
+                if (lane == 0) {
+                    s_fault = 1;
+                    if (g.fault) atomicOr(g.fault, 1u);
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int m0 = tile * kTcRows;
+            const int valid = min(kTcRows, M - m0);
+            const int r = warp * 32 + lane;
+            const long long row = (long long)m0 + r;
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                uint32_t v[16];
+                const uint32_t src = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)a * acc_cols + (uint32_t)c0;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(src));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (r < valid) {
+                    float f[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        f[j] = __uint_as_float(v[j]) +
+                               ((kEpi == kEpiBiasReluBf16 || kEpi == kEpiBiasF32) ? g.bias[c0 + j] : 0.0f);
+                    if (kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) {
+                        __align__(16) __nv_bfloat16 o[16];
+                        if (kEpi == kEpiBiasReluBf16) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(fmaxf(f[j], 0.0f));
+                        } else {
+                            __align__(16) __nv_bfloat16 mk[16];
+                            const uint4 *ms = reinterpret_cast<const uint4 *>(g.mask + row * g.ldm + c0);
+                            reinterpret_cast<uint4 *>(mk)[0] = ms[0];
+                            reinterpret_cast<uint4 *>(mk)[1] = ms[1];
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                o[j] = __float2bfloat16(__bfloat162float(mk[j]) > 0.0f ? f[j] : 0.0f);
+                        }
+                        uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) + row * g.ldc + c0);
+                        dst[0] = reinterpret_cast<const uint4 *>(o)[0];
+                        dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+                    } else {
+                        float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(g.C) +
+                                                                 (long long)blockIdx.y * g.c_split + row * g.ldc + c0);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            dst[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                    }
+                }
+            }
+            // this warp's reads of the accumulator are done: release it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) tc_mbar_arrive(acce0 + 8u * a);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols));
+}
+
 }  // namespace sg
 }  // namespace fd2

@@ -373,6 +373,10 @@ GemmArgs gemm_args(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int 
 
 }  // namespace
 
+namespace {
+cudaError_t launch_tc(fd2_sg *s, cudaStream_t st, const TcArgs &t, unsigned grid_x, unsigned grid_y);
+}  // namespace
+
 // One forward product (K-contiguous operands, bias epilogue): tcgen05 when
 // the shapes fit one pass of fd2_sg_tc.cuh, else the mma.sync kernel.
 static cudaError_t sg_dense(fd2_sg *s, cudaStream_t st, const GemmArgs &g)
@@ -398,11 +402,7 @@ static cudaError_t sg_dense(fd2_sg *s, cudaStream_t st, const GemmArgs &g)
     t.ldc = g.ldc;
     t.fault = s->d_tc_fault;
     const unsigned grid = (unsigned)std::min((g.M + kTcRows - 1) / kTcRows, s->sm_count);
-    const size_t smem = tc_smem_bytes(g.N, g.K);
-    if (g.epi == kEpiBiasReluBf16) gemm_tc_kernel<kEpiBiasReluBf16><<<grid, kTcThreads, smem, st>>>(t);
-    else if (g.epi == kEpiBiasF32) gemm_tc_kernel<kEpiBiasF32><<<grid, kTcThreads, smem, st>>>(t);
-    else return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    return launch_tc(s, st, t, grid, 1);
 }
 
 fd2_status sg_tc_check(fd2_sg *s)
@@ -473,8 +473,17 @@ cudaError_t launch_transpose(cudaStream_t st, const __nv_bfloat16 *in, int ld_in
 
 cudaError_t launch_tc(fd2_sg *s, cudaStream_t st, const TcArgs &t, unsigned grid_x, unsigned grid_y)
 {
-    const size_t smem = tc_smem_bytes(t.N, t.K);
     const dim3 grid(grid_x, grid_y);
+    if (s->tc_pipe && t.K % 16 == 0 && (t.K <= kPipeChunkK || t.K % kPipeChunkK == 0)) {
+        const size_t smem = tc_pipe_smem_bytes(t.N, t.K);
+        if (t.epi == kEpiBiasReluBf16) gemm_tc_pipe_kernel<kEpiBiasReluBf16><<<grid, kPipeThreads, smem, st>>>(t);
+        else if (t.epi == kEpiBiasF32) gemm_tc_pipe_kernel<kEpiBiasF32><<<grid, kPipeThreads, smem, st>>>(t);
+        else if (t.epi == kEpiMaskBf16) gemm_tc_pipe_kernel<kEpiMaskBf16><<<grid, kPipeThreads, smem, st>>>(t);
+        else if (t.epi == kEpiPartialF32) gemm_tc_pipe_kernel<kEpiPartialF32><<<grid, kPipeThreads, smem, st>>>(t);
+        else return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
+    const size_t smem = tc_smem_bytes(t.N, t.K);
     if (t.epi == kEpiBiasReluBf16) gemm_tc_kernel<kEpiBiasReluBf16><<<grid, kTcThreads, smem, st>>>(t);
     else if (t.epi == kEpiBiasF32) gemm_tc_kernel<kEpiBiasF32><<<grid, kTcThreads, smem, st>>>(t);
     else if (t.epi == kEpiMaskBf16) gemm_tc_kernel<kEpiMaskBf16><<<grid, kTcThreads, smem, st>>>(t);
@@ -835,6 +844,7 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
             s->sm_count = sms;
         const char *env = std::getenv("FD2_SG_GEMM");
         s->use_tc = !(env && std::strcmp(env, "mma") == 0);
+        s->tc_pipe = !(env && std::strcmp(env, "tc1") == 0);
         // the tcgen05 kernels' shared memory (outside any stream capture)
         const int bytes = (int)tc_smem_bytes(kTcMaxN, kTcMaxK);
         if (cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasReluBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
@@ -845,6 +855,16 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
                 cudaSuccess ||
             cudaFuncSetAttribute(gemm_tc_kernel<kEpiPartialF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
                 cudaSuccess)
+            return bail(FD2_ERR_CUDA);
+        const int pbytes = (int)tc_pipe_smem_bytes(kTcMaxN, kTcMaxK);
+        if (cudaFuncSetAttribute(gemm_tc_pipe_kernel<kEpiBiasReluBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 pbytes) != cudaSuccess ||
+            cudaFuncSetAttribute(gemm_tc_pipe_kernel<kEpiBiasF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, pbytes) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(gemm_tc_pipe_kernel<kEpiMaskBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 pbytes) != cudaSuccess ||
+            cudaFuncSetAttribute(gemm_tc_pipe_kernel<kEpiPartialF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 pbytes) != cudaSuccess)
             return bail(FD2_ERR_CUDA);
     }
     const std::vector<uint8_t> live = live_mask(s);

@@ -196,3 +196,30 @@ def test_tensor_core_backward_matches_mma_sync(require_gpu, monkeypatch):
         rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
         cos = a @ b / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-30)
         assert np.all(np.isfinite(a)) and rel < 1e-2 and cos > 0.9999, (name, rel, cos)
+
+
+def test_pipelined_tensor_core_kernel_equals_simple(require_gpu, monkeypatch):
+    """The default tcgen05 kernel overlaps the loads of the next chunks and
+    the epilogue of the previous tile with the MMAs (producer warp, MMA
+    thread, four epilogue warps, mbarrier ring, two TMEM accumulators); the
+    one-tile-at-a-time kernel (FD2_SG_GEMM=tc1) issues the same MMAs in the
+    same order, so forward outputs and gradients are bitwise equal.  Ragged
+    sizes: 9,000 prediction rows (70 full tiles and a partial one), 3,000
+    training rows (12 batch slices)."""
+    H = 256
+    p, f, lo, hi, ph, de, ra = _random_problem(23, 9000, H)
+    res = []
+    for mode in ("pipe", "tc1"):
+        if mode == "tc1":
+            monkeypatch.setenv("FD2_SG_GEMM", "tc1")
+        else:
+            monkeypatch.delenv("FD2_SG_GEMM", raising=False)
+        with sgm.Surrogate(hidden=H, batch=4096, radial_bins=64, radial_max_um=200.0) as s:
+            s.set_params(p)
+            s.set_hull(lo, hi)
+            out = s.predict(f)
+            loss, g = s.loss_grad(f[:3000], ph[:3000], de[:3000], ra[:3000])
+        res.append((out, loss, g))
+    (oa, la, ga), (ob, lb, gb) = res
+    assert np.all(np.isfinite(oa)) and np.array_equal(oa, ob)
+    assert la == lb and np.array_equal(ga, gb)
