@@ -264,12 +264,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 
 // ---------------------------------------------------------------------------
 // Pipelined variant: the same products with the stages of consecutive tiles
-// overlapped.  Six warps with fixed roles:
-//   warp 4 (producer): stages A in 128-row x 64-K chunks (16 KB) into a ring
-//     of four shared-memory stages with cp.async, then fence.proxy.async and
-//     an arrive on the stage's `full` barrier; it waits on the stage's
-//     `empty` barrier (the MMAs that read it have completed) before reuse;
-//   warp 5 (one elected thread): issues the tcgen05.mma of each chunk as soon
+// overlapped.  Seven warps with fixed roles:
+//   warps 4-5 (producers): stage A in 128-row x 64-K chunks (16 KB) into a ring
+//     of four shared-memory stages with cp.async, three chunks in flight;
+//     once a chunk's copies have completed, fence.proxy.async and an arrive
+//     on its stage's `full` barrier; it waits on the stage's `empty` barrier
+//     (the MMAs that read it have completed) before reuse;
+//   warp 6 (one elected thread): issues the tcgen05.mma of each chunk as soon
 //     as its stage is full, commits each stage to its `empty` barrier and each
 //     finished tile to its accumulator's `accf` barrier; two TMEM
 //     accumulators alternate between tiles, and a tile starts only when the
@@ -284,7 +285,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 // MMAs are the simple kernel's, in the same order, so the results are
 // bitwise identical to it.
 constexpr int kPipeStages = 4;
-constexpr int kPipeThreads = 192;
+constexpr int kPipeDepth = 3;  // chunks a producer lane keeps in flight (< kPipeStages)
+constexpr int kPipeProducers = 2;  // producer warps
+constexpr int kPipeThreads = 32 * (5 + kPipeProducers);  // 4 epilogue warps, the producers, 1 MMA warp
+constexpr int kPipeMmaWarp = 4 + kPipeProducers;
 constexpr int kPipeChunkK = 64;
 
 __host__ __device__ inline int tc_pipe_chunk(int K) { return K < kPipeChunkK ? K : kPipeChunkK; }
@@ -329,6 +333,26 @@ __device__ __forceinline__ void tc_commit(uint32_t bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+// One 128-row chunk of A (kc = CK / 8 16-byte pieces per row, a power of two)
+// by the producer threads `tid` of `nthr` (a multiple of 8): the same layout
+// as tc_stage, with shifts instead of divisions.
+__device__ __forceinline__ void tc_stage_chunk(unsigned char *dst, const __nv_bfloat16 *src, int ld, int valid, int kc,
+                                               int lg_kc, int tid, int nthr)
+{
+    const int ri = tid & 7;  // fixed for the thread: nthr is a multiple of 8
+    const int total = kTcRows * kc;
+    for (int L = tid; L < total; L += nthr) {
+        const int t = L >> 3;
+        const int c = t & (kc - 1), rg = t >> lg_kc;
+        const int r = rg * 8 + ri;
+        const bool ok = r < valid;
+        const __nv_bfloat16 *gp = src + (long long)(ok ? r : 0) * ld + c * 8;
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + (size_t)c * (kTcRows * 16) + (size_t)rg * 128 +
+                                                               (size_t)ri * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gp), "r"(ok ? 16 : 0) : "memory");
+    }
+}
+
 template <int kEpi>
 __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcArgs g)
 {
@@ -365,7 +389,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
     const uint32_t drain = (uint32_t)__cvta_generic_to_shared(&s_drain);
     if (threadIdx.x == 0) {
         for (int i = 0; i < kPipeStages; ++i) {
-            tc_mbar_init(full0 + 8u * i, 32);  // the producer warp's lanes
+            tc_mbar_init(full0 + 8u * i, 32 * kPipeProducers);  // the producer lanes
             tc_mbar_init(empty0 + 8u * i, 1);  // one tcgen05.commit
         }
         for (int i = 0; i < 2; ++i) {
@@ -384,8 +408,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = s_taddr;
 
-    if (warp == 4) {
-        // ---- producer
+    if (warp >= 4 && warp < kPipeMmaWarp) {
+        // ---- producers: up to kPipeDepth chunks' copies in flight per lane
+        // (cp.async groups); a chunk's stage is marked full once its group
+        // has completed and a proxy fence has made the writes visible to the
+        // tensor core
         int gc = 0;
         bool ok = true;
         for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
@@ -403,14 +430,22 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
                     }
                     break;
                 }
-                tc_stage_part(sRing + (size_t)st * stage_bytes, gA + (long long)m0 * g.lda + c * CK, g.lda, kTcRows,
-                              valid, CK, lane, 32);
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tc_mbar_arrive(full0 + 8u * st);
+                tc_stage_chunk(sRing + (size_t)st * stage_bytes, gA + (long long)m0 * g.lda + c * CK, g.lda, valid,
+                               CK / 8, __ffs(CK / 8) - 1, threadIdx.x - 128, 32 * kPipeProducers);
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                if (gc >= kPipeDepth - 1) {
+                    // chunk gc - (depth - 1) has landed
+                    asm volatile("cp.async.wait_group %0;" ::"n"(kPipeDepth - 1) : "memory");
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    tc_mbar_arrive(full0 + 8u * ((gc - (kPipeDepth - 1)) % kPipeStages));
+                }
             }
         }
-    } else if (warp == 5) {
+        // the chunks still in flight
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (int j = max(gc - (kPipeDepth - 1), 0); j < gc; ++j) tc_mbar_arrive(full0 + 8u * (j % kPipeStages));
+    } else if (warp == kPipeMmaWarp) {
         // ---- MMA issue (one thread)
         if (lane == 0) {
             const uint32_t idesc = tc_instr_desc(kTcRows, N);
