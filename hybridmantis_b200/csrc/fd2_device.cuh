@@ -208,6 +208,29 @@ struct Walker {
         nx = rx * ir; ny = ry * ir; nz = rz * ir;
     }
 
+    // A new column's orientation before its own roughening: (ix, iy, iz)
+    // roughened with beta = 1 and flattened to the x-y plane (the
+    // reference's RoughSurface(1) followed by nz = 0 and a 2D
+    // normalisation).  The 3D normalisation between the two is a positive
+    // scale the 2D one removes, so the flattened direction of i + q/|q| is
+    // taken directly; the draws are roughen's.
+    __device__ __forceinline__ void flat_rough(float ix, float iy, float iz)
+    {
+        const float u1 = u();
+        const float qz = 2.0f * u1 - 1.0f;
+        const float rr = sqrtf(fmaxf(0.0f, 1.0f - u1 * u1));
+        float s, c;
+        __sincosf(kPi * (2.0f * u() - 1.0f), &s, &c);
+        const float qx = rr * c, qy = rr * s;
+        const float iq = rsqrtf(qx * qx + qy * qy + qz * qz);
+        const float vx = fmaf(iq, qx, ix), vy = fmaf(iq, qy, iy);
+        const float inv = rsqrtf(vx * vx + vy * vy);
+        nx = vx * inv;
+        ny = vy * inv;
+        nz = 0.0f;
+        (void)iz;
+    }
+
     template <class G>
     __device__ __forceinline__ bool outside_xy(const G &g) const
     {
@@ -300,10 +323,7 @@ struct Walker {
                                                      bool always_rough)
     {
         for (;;) {
-            nx = ix; ny = iy; nz = iz;
-            roughen(1.0f);
-            const float inv = rsqrtf(nx * nx + ny * ny);
-            nx *= inv; ny *= inv; nz = 0.0f;
+            flat_rough(ix, iy, iz);
             if (always_rough || g.beta > 0.0f) roughen(g.beta);
             if (!(ix * nx + iy * ny + iz * nz < kCos157)) return kAlive;
             if (tries < 100) {
@@ -473,10 +493,7 @@ struct Walker {
     __device__ __forceinline__ int crosstalk_normal(const G &g, int &tries)
     {
         const float ix = -dx, iy = -dy, iz = -dz;
-        nx = ix; ny = iy; nz = iz;
-        roughen(1.0f);
-        const float inv = rsqrtf(nx * nx + ny * ny);
-        nx *= inv; ny *= inv; nz = 0.0f;
+        flat_rough(ix, iy, iz);
         if (g.beta > 0.0f) roughen(g.beta);
         if (!(ix * nx + iy * ny + iz * nz < kCos157)) {
             xc = fmaf(-g.R, nx, px);
