@@ -202,7 +202,8 @@ struct Walker {
         float s, c;
         __sincosf(kPi * (2.0f * u() - 1.0f), &s, &c);
         const float qx = rr * c, qy = rr * s;
-        const float bq = beta * rsqrtf(qx * qx + qy * qy + qz * qz);
+        // |q|^2 = (1 - u1^2) + (2 u1 - 1)^2 = 3 u1^2 - 4 u1 + 2 for u1 in (0, 1)
+        const float bq = beta * rsqrtf(fmaf(u1, fmaf(3.0f, u1, -4.0f), 2.0f));
         const float rx = fmaf(bq, qx, nx), ry = fmaf(bq, qy, ny), rz = fmaf(bq, qz, nz);
         const float ir = rsqrtf(rx * rx + ry * ry + rz * rz);
         nx = rx * ir; ny = ry * ir; nz = rz * ir;
@@ -222,7 +223,7 @@ struct Walker {
         float s, c;
         __sincosf(kPi * (2.0f * u() - 1.0f), &s, &c);
         const float qx = rr * c, qy = rr * s;
-        const float iq = rsqrtf(qx * qx + qy * qy + qz * qz);
+        const float iq = rsqrtf(fmaf(u1, fmaf(3.0f, u1, -4.0f), 2.0f));  // 1 / |q|, as in roughen
         const float vx = fmaf(iq, qx, ix), vy = fmaf(iq, qy, iy);
         const float inv = rsqrtf(vx * vx + vy * vy);
         nx = vx * inv;
