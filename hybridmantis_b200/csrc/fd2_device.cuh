@@ -335,47 +335,34 @@ struct Walker {
         }
     }
 
-    // Hop after a specular reflection on the sensor between columns
-    // (refl_bottom): up to the top, or to a new column.
-    template <class G>
-    __device__ __forceinline__ int sensor_hop(const G &g)
-    {
-        const float sx = px, sy = py, sz = pz;
-        const float ix = -dx, iy = -dy, iz = -dz;
-        const float hop = fmaf(u(), g.d_span, g.d_min);
-        const float dtop = (g.half - sz) / dz;
-        px = fmaf(dx, hop, sx);
-        py = fmaf(dy, hop, sy);
-        pz = fmaf(dz, hop, sz);
-        if (outside_xy(g)) return kLost;
-        if (pz > g.half) {
-            if (dtop < hop && dtop > kEps) {
-                px = fmaf(dx, dtop, sx);
-                py = fmaf(dy, dtop, sy);
-                pz = g.half;
-                dist += dtop;
-                return kAlive;
-            }
-            return kLost;
-        }
-        dist += hop;
-        int tries = 0;
-        return new_column_normal(g, ix, iy, iz, tries, true);
-    }
-
     // Leave the current column after a transmission through its wall
     // (transmit without crosstalk; crosstalk is crosstalk_normal): hop
     // U(d_min, d_max) with the top reflector and the sensor on the way, then
     // orient the next column.  Hops after a top reflection repeat the loop.
+    // A photon reflected by the sensor between columns hops again
+    // (refl_bottom): up to the top, or into a new column whose normal is
+    // drawn around its own reversed direction, always roughened; after a
+    // sensor met at the hop's end it stays where that hop left it unless it
+    // reached the top.
+    // Written as a state machine so that the kernel holds one copy of each
+    // part (hop, sensor, hop after the sensor, next normal, top reflector):
+    // the walk's instruction fetch grows with the kernel's code size.
     template <class G>
     __device__ __forceinline__ int leave_column(const G &g)
     {
-        float ix = -dx, iy = -dy, iz = -dz;
-        int tries = 0, tries_top = 0;
-        bool side_hop = true;
-        for (int loop = 0; loop < kMaxTopLoops; ++loop) {
-            bool sensor_hit = false;
-            {
+        enum { kHop, kSensor, kSensorHop, kNormal, kAfterSensor, kEnd };
+        float ix = -dx, iy = -dy, iz = -dz;  // the next normal is drawn around these
+        // One register for the rest: retries of the side hop's and the top
+        // hops' normals (bits 0-7 and 8-15, each at most 100), top
+        // reflections (bits 16-28, at most kMaxTopLoops), and three flags.
+        constexpr uint32_t kSideHop = 1u << 29;     // the hop leaves a column wall (not the top)
+        constexpr uint32_t kFromEnd = 1u << 30;     // the sensor was met at a hop's end, not during it
+        constexpr uint32_t kAfterHop = 1u << 31;    // the pending normal follows a sensor hop
+        constexpr uint32_t kTopOne = 1u << 16, kTopMask = 0x1fffu << 16;
+        uint32_t counts = kSideHop;
+        int st = kHop;
+        for (;;) {
+            if (st == kHop) {
                 const float sx = px, sy = py, sz = pz;
                 const float d = fmaf(u(), g.d_span, g.d_min);
                 px = fmaf(dx, d, sx);
@@ -384,6 +371,8 @@ struct Walker {
                 const float dtop = (g.half - sz) / dz;
                 const float dbot = (-g.half - sz) / dz;
                 if (outside_xy(g)) return kLost;
+                counts &= ~kAfterHop;
+                st = kNormal;
                 if (pz < -g.half || pz > g.half) {
                     if (dtop < d && dtop > kEps) {
                         px = fmaf(dx, dtop, sx);
@@ -395,16 +384,15 @@ struct Walker {
                         py = fmaf(dy, dbot, sy);
                         pz = -g.half;
                         dist += dbot;
-                        sensor_hit = true;
+                        counts &= ~kFromEnd;
+                        st = kSensor;
                     } else {
                         return kLost;
                     }
                 } else {
                     dist += d;
                 }
-            }
-            bool up_to_top = false;
-            if (sensor_hit) {
+            } else if (st == kSensor) {
                 // sensor between columns: reflect with sensorRefl, else detect
                 if (!(g.sensor_refl > 0.0f && u() < g.sensor_refl)) {
                     set_pixel(g);
@@ -412,20 +400,61 @@ struct Walker {
                 }
                 dz = -dz;
                 renorm(dx, dy, dz);
-                const int f = sensor_hop(g);
+                st = kSensorHop;
+            } else if (st == kSensorHop) {
+                const float sx = px, sy = py, sz = pz;
+                const float hop = fmaf(u(), g.d_span, g.d_min);
+                const float dtop = (g.half - sz) / dz;
+                px = fmaf(dx, hop, sx);
+                py = fmaf(dy, hop, sy);
+                pz = fmaf(dz, hop, sz);
+                if (outside_xy(g)) return kLost;
+                if (pz > g.half) {
+                    if (!(dtop < hop && dtop > kEps)) return kLost;
+                    px = fmaf(dx, dtop, sx);
+                    py = fmaf(dy, dtop, sy);
+                    pz = g.half;
+                    dist += dtop;
+                    st = kAfterSensor;
+                } else {
+                    dist += hop;
+                    counts |= kAfterHop;
+                    st = kNormal;
+                }
+            } else if (st == kNormal) {
+                const bool after_sensor = (counts & kAfterHop) != 0u, side_hop = (counts & kSideHop) != 0u;
+                int t = after_sensor ? 0 : (int)((side_hop ? counts : counts >> 8) & 0xffu);
+                // after a sensor hop: around the hop's own reversed direction
+                const float ax = after_sensor ? -dx : ix, ay = after_sensor ? -dy : iy, az = after_sensor ? -dz : iz;
+                const int f = new_column_normal(g, ax, ay, az, t, after_sensor);
                 if (f != kAlive) return f;
-                up_to_top = at_top(g);
-            }
-            if (!up_to_top) {
-                const int f = new_column_normal(g, ix, iy, iz, side_hop ? tries : tries_top, false);
-                if (f != kAlive) return f;
-                if (side_hop && (fabsf(px) < kEps || fabsf(px - g.xdet) < kEps || fabsf(py) < kEps ||
-                                 fabsf(py - g.ydet) < kEps))
-                    return kLost;
-            }
-            // top reflector / sensor at the end of the hop
-            bool again = false;
-            for (int k = 0; k < kMaxTopLoops; ++k) {
+                if (after_sensor) {
+                    st = kAfterSensor;
+                } else {
+                    counts = side_hop ? (counts & ~0xffu) | (uint32_t)t : (counts & ~0xff00u) | ((uint32_t)t << 8);
+                    if (side_hop && (fabsf(px) < kEps || fabsf(px - g.xdet) < kEps || fabsf(py) < kEps ||
+                                     fabsf(py - g.ydet) < kEps))
+                        return kLost;
+                    st = kEnd;
+                }
+            } else if (st == kAfterSensor) {
+                counts &= ~kAfterHop;
+                if (!(counts & kFromEnd)) {
+                    // a sensor met during the hop: the next normal follows
+                    // unless the sensor hop reached the top
+                    if (at_top(g)) {
+                        st = kEnd;
+                    } else {
+                        st = kNormal;
+                    }
+                } else {
+                    // a sensor hop that reached the top ends at the top
+                    // reflector (the hop's end check finds the top at once)
+                    if (!at_top(g)) return kAlive;
+                    st = kEnd;
+                }
+            } else {
+                // kEnd: top reflector / sensor at the end of the hop
                 if (at_top(g)) {
                     if (g.top_absfrac > 0.0f && u() < g.top_absfrac) return kAbsTop;
                     dz = -fabsf(2.0f * u() - 1.0f);
@@ -435,24 +464,16 @@ struct Walker {
                     dx = rr * c;
                     dy = rr * s;
                     ix = -dx; iy = -dy; iz = -dz;
-                    again = true;
-                    break;
+                    counts = (counts & ~kSideHop) + kTopOne;
+                    if ((counts & kTopMask) == ((uint32_t)kMaxTopLoops << 16)) return kCapped;
+                    st = kHop;
+                } else {
+                    if (fabsf(pz + g.half) >= kEps) return kAlive;
+                    counts |= kFromEnd;
+                    st = kSensor;
                 }
-                if (fabsf(pz + g.half) >= kEps) return kAlive;
-                if (!(g.sensor_refl > 0.0f && u() < g.sensor_refl)) {
-                    set_pixel(g);
-                    return kDetect;
-                }
-                dz = -dz;
-                renorm(dx, dy, dz);
-                const int f = sensor_hop(g);
-                if (f != kAlive) return f;
-                if (!at_top(g)) return kAlive;
             }
-            if (!again) return kCapped;
-            side_hop = false;
         }
-        return kCapped;
     }
 
     // Interaction with a surface (boundary_analysis), first part: the top
@@ -943,9 +964,14 @@ struct Walker {
     template <class G>
     __device__ __forceinline__ int step(const G &g, const float4 &event)
     {
-        int f = flight(g);
-        if (f != kAlive) return f;
-        if (fabsf(pz + g.half) < kEps) {
+        // one flight, and a second after a specular reflection on the sensor
+        // inside a column (a loop, so that the kernel holds one flight)
+        bool reflected = false;
+#pragma unroll 1
+        for (;;) {
+            const int f = flight(g);
+            if (f != kAlive) return f;
+            if (reflected || !(fabsf(pz + g.half) < kEps)) break;
             // sensor plane inside a column (detection)
             if (!(g.sensor_refl > 0.0f && u() < g.sensor_refl)) {
                 set_pixel(g);
@@ -953,8 +979,7 @@ struct Walker {
             }
             dz = -dz;  // specular reflection on the flat sensor
             renorm(dx, dy, dz);
-            f = flight(g);
-            if (f != kAlive) return f;
+            reflected = true;
         }
         if (fabsf(dz) < kEps) {
             // trapped travelling horizontally: restart from the event position,
