@@ -287,9 +287,9 @@ TRANSPORT_DRAM_BYTES_PER_PHOTON = 0.57
 # inst_executed), warp instructions per photon (smsp__inst_executed.sum /
 # photons) and the tallies' L2 reductions against their peak
 # (lts__t_sectors_op_red.avg.pct_of_peak_sustained_elapsed).
-TRANSPORT_NCU = {"issue_slot_utilisation": 0.747, "fp32_pipe_utilisation": 0.283,
-                 "lanes_per_instruction": 16.26, "warp_instructions_per_photon": 1174.2,
-                 "l2_reduction_pct_of_peak": 0.60,
+TRANSPORT_NCU = {"issue_slot_utilisation": 0.851, "fp32_pipe_utilisation": 0.334,
+                 "lanes_per_instruction": 16.03, "warp_instructions_per_photon": 1233.4,
+                 "l2_reduction_pct_of_peak": 0.66,
                  "source": "ncu --clock-control none on 20,000 config-1 x-rays "
                            "(transport_kernel<false,256,4,false,false,false>, default launch)"}
 

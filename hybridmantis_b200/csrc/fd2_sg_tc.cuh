@@ -276,7 +276,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 //     accumulators alternate between tiles, and a tile starts only when the
 //     epilogue has released its accumulator (`acce`);
 //   warps 0-3 (epilogue): drain their 32 TMEM lanes of a finished accumulator
-//     (tcgen05.ld), apply the epilogue, store, release the accumulator.
+//     (tcgen05.ld, four loads of 16 columns in flight per wait), apply the
+//     epilogue (bias from shared memory), store, release the accumulator.
+//     BF16 outputs (and the ReLU mask they read) pass through a 32-row x
+//     128-byte tile per warp in shared memory, its 16-byte pieces XOR-swizzled
+//     by row so that neither the row-per-lane side nor the coalesced side has
+//     bank conflicts: a warp's global store then writes four whole 128-byte
+//     row segments instead of 16 bytes of 32 rows.
 // So the loads of the next chunks and the epilogue of the previous tile run
 // while the tensor core works.  B stays resident as before.  Every wait is
 // bounded (tc_wait); a role that gives up sets the fault word and leaves its
@@ -293,12 +299,29 @@ constexpr int kPipeChunkK = 64;
 
 __host__ __device__ inline int tc_pipe_chunk(int K) { return K < kPipeChunkK ? K : kPipeChunkK; }
 
-// Dynamic shared memory of one CTA: B + the A ring.
+constexpr int kPipeOutBytes = 32 * 128;  // an epilogue warp's output tile: 32 rows x 64 BF16 columns
+
+// Dynamic shared memory of one CTA: B + the A ring + the epilogue warps'
+// output tiles.
 __host__ __device__ inline size_t tc_pipe_smem_bytes(int N, int K)
 {
     return (size_t)N * (size_t)K * sizeof(__nv_bfloat16) +
-           (size_t)kPipeStages * kTcRows * (size_t)tc_pipe_chunk(K) * sizeof(__nv_bfloat16);
+           (size_t)kPipeStages * kTcRows * (size_t)tc_pipe_chunk(K) * sizeof(__nv_bfloat16) + 4 * kPipeOutBytes;
 }
+
+// 16 TMEM columns of the warp's 32 lanes (no wait).
+__device__ __forceinline__ void tc_ld16(uint32_t src, uint32_t *v)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+        "%13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(src));
+}
+
+// Byte offset of 16-byte piece c (0-7) of row r in a warp's output tile.
+__device__ __forceinline__ uint32_t tc_out_off(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
 
 // tc_stage for thread `tid` of `nthr` (a subset of the CTA).
 __device__ __forceinline__ void tc_stage_part(unsigned char *dst, const __nv_bfloat16 *src, int ld, int rows,
@@ -361,6 +384,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
         s_drain;
     __shared__ uint32_t s_taddr;
     __shared__ int s_fault;
+    __shared__ __align__(16) float s_bias[kTcMaxN];
+    constexpr bool kBias = kEpi == kEpiBiasReluBf16 || kEpi == kEpiBiasF32;
 
     int M = g.M;
     if (g.m_limit) M = min(M, *g.m_limit);
@@ -374,6 +399,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
     unsigned char *sB = tc_smem;
     unsigned char *sRing = tc_smem + (size_t)N * K * 2;
     const uint32_t stage_bytes = (uint32_t)(kTcRows * CK * 2);
+    unsigned char *sOut = sRing + (size_t)kPipeStages * stage_bytes;
     const uint32_t acc_cols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
     const uint32_t cols = 2u * acc_cols;
 
@@ -401,6 +427,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
     }
     // B stays resident for all of the CTA's tiles
     tc_stage_part(sB, gB, g.ldb, N, N, K, threadIdx.x, blockDim.x);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s_bias[i] = kBias ? g.bias[i] : 0.0f;
     asm volatile("cp.async.wait_all;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -517,46 +544,97 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
             const int valid = min(kTcRows, M - m0);
             const int r = warp * 32 + lane;
             const long long row = (long long)m0 + r;
-            for (int c0 = 0; c0 < N; c0 += 16) {
-                uint32_t v[16];
-                const uint32_t src = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)a * acc_cols + (uint32_t)c0;
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                    "%13, %14, %15}, [%16];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                      "=r"(v[15])
-                    : "r"(src));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (r < valid) {
-                    float f[16];
+            const uint32_t tsrc = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)a * acc_cols;
+            if ((kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) && (N & 63) == 0) {
+                // 64 columns at a time through the warp's output tile
+                unsigned char *out = sOut + (size_t)warp * kPipeOutBytes;
+                for (int c0 = 0; c0 < N; c0 += 64) {
+                    uint32_t v[64];
+                    tc_ld16(tsrc + (uint32_t)c0, v);
+                    tc_ld16(tsrc + (uint32_t)c0 + 16u, v + 16);
+                    tc_ld16(tsrc + (uint32_t)c0 + 32u, v + 32);
+                    tc_ld16(tsrc + (uint32_t)c0 + 48u, v + 48);
+                    if (kEpi == kEpiMaskBf16) {
+                        // the mask's 32 x 64 block, read coalesced while the TMEM loads run
 #pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        f[j] = __uint_as_float(v[j]) +
-                               ((kEpi == kEpiBiasReluBf16 || kEpi == kEpiBiasF32) ? g.bias[c0 + j] : 0.0f);
-                    if (kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) {
-                        __align__(16) __nv_bfloat16 o[16];
+                        for (int i = 0; i < 8; ++i) {
+                            const int rr = 4 * i + (lane >> 3), c = lane & 7;
+                            uint4 mv = make_uint4(0u, 0u, 0u, 0u);
+                            if (warp * 32 + rr < valid)
+                                mv = *reinterpret_cast<const uint4 *>(g.mask + ((long long)m0 + warp * 32 + rr) * g.ldm +
+                                                                      c0 + c * 8);
+                            *reinterpret_cast<uint4 *>(out + tc_out_off(rr, c)) = mv;
+                        }
+                        __syncwarp();
+                    }
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    // piece jc of the lane's own row: its mask is read from, and its
+                    // output written to, the same place, by this lane only
+#pragma unroll
+                    for (int jc = 0; jc < 8; ++jc) {
+                        const float4 b0 = *reinterpret_cast<const float4 *>(&s_bias[c0 + 8 * jc]);
+                        const float4 b1 = *reinterpret_cast<const float4 *>(&s_bias[c0 + 8 * jc + 4]);
+                        const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                        __align__(16) __nv_bfloat16 o[8];
                         if (kEpi == kEpiBiasReluBf16) {
 #pragma unroll
-                            for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(fmaxf(f[j], 0.0f));
+                            for (int j = 0; j < 8; ++j)
+                                o[j] = __float2bfloat16(fmaxf(__uint_as_float(v[8 * jc + j]) + bb[j], 0.0f));
                         } else {
-                            __align__(16) __nv_bfloat16 mk[16];
-                            const uint4 *ms = reinterpret_cast<const uint4 *>(g.mask + row * g.ldm + c0);
-                            reinterpret_cast<uint4 *>(mk)[0] = ms[0];
-                            reinterpret_cast<uint4 *>(mk)[1] = ms[1];
+                            __align__(16) __nv_bfloat16 mk[8];
+                            *reinterpret_cast<uint4 *>(mk) = *reinterpret_cast<const uint4 *>(out + tc_out_off(lane, jc));
 #pragma unroll
-                            for (int j = 0; j < 16; ++j)
-                                o[j] = __float2bfloat16(__bfloat162float(mk[j]) > 0.0f ? f[j] : 0.0f);
+                            for (int j = 0; j < 8; ++j) {
+                                const float f = __uint_as_float(v[8 * jc + j]) + bb[j];
+                                o[j] = __float2bfloat16(__bfloat162float(mk[j]) > 0.0f ? f : 0.0f);
+                            }
                         }
-                        uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) + row * g.ldc + c0);
-                        dst[0] = reinterpret_cast<const uint4 *>(o)[0];
-                        dst[1] = reinterpret_cast<const uint4 *>(o)[1];
-                    } else {
-                        float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(g.C) +
-                                                                 (long long)blockIdx.y * g.c_split + row * g.ldc + c0);
+                        *reinterpret_cast<uint4 *>(out + tc_out_off(lane, jc)) = *reinterpret_cast<const uint4 *>(o);
+                    }
+                    __syncwarp();
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                            dst[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                    for (int i = 0; i < 8; ++i) {
+                        const int rr = 4 * i + (lane >> 3), c = lane & 7;
+                        const uint4 val = *reinterpret_cast<const uint4 *>(out + tc_out_off(rr, c));
+                        if (warp * 32 + rr < valid)
+                            *reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) +
+                                                       ((long long)m0 + warp * 32 + rr) * g.ldc + c0 + c * 8) = val;
+                    }
+                    __syncwarp();  // the tile is read before the next columns overwrite it
+                }
+            } else {
+                for (int c0 = 0; c0 < N; c0 += 16) {
+                    uint32_t v[16];
+                    tc_ld16(tsrc + (uint32_t)c0, v);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (r < valid) {
+                        float f[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) f[j] = __uint_as_float(v[j]) + s_bias[c0 + j];
+                        if (kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) {
+                            __align__(16) __nv_bfloat16 o[16];
+                            if (kEpi == kEpiBiasReluBf16) {
+#pragma unroll
+                                for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16(fmaxf(f[j], 0.0f));
+                            } else {
+                                __align__(16) __nv_bfloat16 mk[16];
+                                const uint4 *ms = reinterpret_cast<const uint4 *>(g.mask + row * g.ldm + c0);
+                                reinterpret_cast<uint4 *>(mk)[0] = ms[0];
+                                reinterpret_cast<uint4 *>(mk)[1] = ms[1];
+#pragma unroll
+                                for (int j = 0; j < 16; ++j)
+                                    o[j] = __float2bfloat16(__bfloat162float(mk[j]) > 0.0f ? f[j] : 0.0f);
+                            }
+                            uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) + row * g.ldc + c0);
+                            dst[0] = reinterpret_cast<const uint4 *>(o)[0];
+                            dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+                        } else {
+                            float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(g.C) +
+                                                                     (long long)blockIdx.y * g.c_split + row * g.ldc + c0);
+#pragma unroll
+                            for (int j = 0; j < 4; ++j)
+                                dst[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                        }
                     }
                 }
             }
