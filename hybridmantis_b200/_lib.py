@@ -184,6 +184,7 @@ EXPORTED = [
     "fd2_sg_default_config", "fd2_sg_create", "fd2_sg_destroy", "fd2_sg_last_error", "fd2_sg_set_data",
     "fd2_sg_train", "fd2_sg_set_lr", "fd2_sg_eval", "fd2_sg_num_params", "fd2_sg_get_params", "fd2_sg_set_params",
     "fd2_sg_get_hull", "fd2_sg_set_hull", "fd2_sg_save", "fd2_sg_load", "fd2_sg_loss_grad", "fd2_sg_predict",
+    "fd2_sg_set_edge", "fd2_sg_get_edge",
     "fd2_sg_run",
     "fd2_mtf", "fd2_nnps",
     "fd2_submit_events_device",
@@ -269,6 +270,8 @@ def load():
         "fd2_sg_set_hull": (ctypes.c_int, [vp, P(SgHull)]),
         "fd2_sg_save": (ctypes.c_int, [vp, ctypes.c_char_p]),
         "fd2_sg_load": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "fd2_sg_set_edge": (ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
+        "fd2_sg_get_edge": (ctypes.c_int, [vp, P(ctypes.c_float), P(ctypes.c_float)]),
         "fd2_sg_loss_grad": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int32, P(ctypes.c_float), vp]),
         "fd2_sg_predict": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp]),
         "fd2_sg_run": (ctypes.c_int, [vp, vp, ctypes.c_double, P(SgStats)]),

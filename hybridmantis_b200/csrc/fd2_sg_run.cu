@@ -173,6 +173,7 @@ struct SampleArgs {
     uint32_t k0, k1;
     int64_t event_base;
     const uint32_t *run_tag;
+    float edge_amp, edge_inv_len;  // edge survival of the azimuths (amplitude 0: off)
 };
 
 constexpr uint32_t kDomainRetry = 0x52455452u;  // rejection retries of ring_radius
@@ -263,8 +264,13 @@ __global__ void sample_kernel(const SampleArgs a)
         }
         const int32_t total = __shfl_sync(0xffffffffu, before, 31);
         // ---- positions of the detected photons: a ring component by weight,
-        // its radius drawn exactly (ring_radius), an azimuth uniform over the
-        // directions that keep the photon on the detector
+        // its radius drawn exactly (ring_radius), an azimuth over the
+        // directions that keep the photon on the detector, uniform or (with an
+        // edge amplitude a > 0) accepted with probability
+        //   W = prod over the four sides (1 - a exp(-s / len)),
+        // s the point's distance to the side: the detected light thins out
+        // towards the detector's sides, whose crossing loses a photon.  Only
+        // the azimuth is redrawn, so the radius keeps the network's law.
         Mix m;
         decode_mix(o, m);
         float cumw[kComponents];
@@ -290,10 +296,21 @@ __global__ void sample_kernel(const SampleArgs a)
             sincospif(2.0f * unit(h.z), &sn, &cs);
             for (uint32_t k = 0; k < 32; ++k) {
                 const float tx = pos.x + rad * cs, ty = pos.y + rad * sn;
-                if (tx >= 0.0f && tx <= g.xdet && ty >= 0.0f && ty <= g.ydet) break;
-                const uint4 hk =
-                    philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainTurn, run * 32u + k),
-                             a.k0, a.k1);
+                bool ok = tx >= 0.0f && tx <= g.xdet && ty >= 0.0f && ty <= g.ydet;
+                // attempt k's acceptance uniform and attempt k + 1's azimuth
+                uint4 hk = make_uint4(0u, 0u, 0u, 0u);
+                const bool draw = !ok || a.edge_amp > 0.0f;
+                if (draw)
+                    hk = philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainTurn, run * 32u + k),
+                                  a.k0, a.k1);
+                if (ok && a.edge_amp > 0.0f) {
+                    const float W = (1.0f - a.edge_amp * __expf(-tx * a.edge_inv_len)) *
+                                    (1.0f - a.edge_amp * __expf(-(g.xdet - tx) * a.edge_inv_len)) *
+                                    (1.0f - a.edge_amp * __expf(-ty * a.edge_inv_len)) *
+                                    (1.0f - a.edge_amp * __expf(-(g.ydet - ty) * a.edge_inv_len));
+                    ok = unit(hk.y) < W;
+                }
+                if (ok) break;
                 sincospif(2.0f * unit(hk.x), &sn, &cs);
             }
             const float x = pos.x + rad * cs, y = pos.y + rad * sn;
@@ -466,6 +483,8 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
         a.k1 = k1;
         a.event_base = c->opt.event_base;
         a.run_tag = reinterpret_cast<const uint32_t *>(c->d_flags + 1);
+        a.edge_amp = s->edge_amp;
+        a.edge_inv_len = 1.0f / s->edge_len_um;
         sample_kernel<<<(unsigned)(c->sm_count * 8), 256, 0, q>>>(a);
         e = cudaGetLastError();
     }

@@ -961,6 +961,23 @@ fd2_status fd2_sg_get_hull(fd2_sg *s, fd2_sg_hull *h)
     return FD2_OK;
 }
 
+fd2_status fd2_sg_set_edge(fd2_sg *s, float amplitude, float length_um)
+{
+    if (!s || !(amplitude >= 0.0f && amplitude < 1.0f) || !(length_um > 0.0f) || !std::isfinite(length_um))
+        return FD2_ERR_INVALID_ARGUMENT;
+    s->edge_amp = amplitude;
+    s->edge_len_um = length_um;
+    return FD2_OK;
+}
+
+fd2_status fd2_sg_get_edge(const fd2_sg *s, float *amplitude, float *length_um)
+{
+    if (!s || !amplitude || !length_um) return FD2_ERR_INVALID_ARGUMENT;
+    *amplitude = s->edge_amp;
+    *length_um = s->edge_len_um;
+    return FD2_OK;
+}
+
 fd2_status fd2_sg_set_hull(fd2_sg *s, const fd2_sg_hull *h)
 {
     if (!s || !h) return FD2_ERR_INVALID_ARGUMENT;
@@ -1171,7 +1188,8 @@ fd2_status fd2_sg_predict(fd2_sg *s, const float *features, int64_t n, float *ou
 }
 
 // File: "FD2SG002", hidden, bins, radial_max, normalisation box, routing
-// hull, public parameters.
+// hull, public parameters; then, optionally, "EDGE" and the edge survival's
+// amplitude and length (float each; a file without them loads amplitude 0).
 fd2_status fd2_sg_save(fd2_sg *s, const char *path)
 {
     if (!s || !path) return FD2_ERR_INVALID_ARGUMENT;
@@ -1186,6 +1204,10 @@ fd2_status fd2_sg_save(fd2_sg *s, const char *path)
               std::fwrite(&s->norm_box, sizeof s->norm_box, 1, f) == 1 &&
               std::fwrite(&s->hull, sizeof s->hull, 1, f) == 1 &&
               std::fwrite(p.data(), sizeof(float), p.size(), f) == p.size();
+    if (s->edge_amp > 0.0f) {
+        const float edge[2] = {s->edge_amp, s->edge_len_um};
+        ok = ok && std::fwrite("EDGE", 1, 4, f) == 4 && std::fwrite(edge, sizeof edge, 1, f) == 1;
+    }
     ok = (std::fclose(f) == 0) && ok;
     return ok ? FD2_OK : sg_fail(s, FD2_ERR_IO, std::string("write failed: ") + path);
 }
@@ -1205,8 +1227,16 @@ fd2_status fd2_sg_load(fd2_sg *s, const char *path)
               std::fread(&nb, sizeof nb, 1, f) == 1 && std::fread(&h, sizeof h, 1, f) == 1;
     ok = ok && hdr[0] == s->hidden && hdr[1] == s->bins && rmax == s->radial_max &&
          std::fread(p.data(), sizeof(float), p.size(), f) == p.size();
+    float edge[2] = {0.0f, 1.0f};
+    char tag[4];
+    if (ok && std::fread(tag, 1, 4, f) == 4) {
+        ok = std::memcmp(tag, "EDGE", 4) == 0 && std::fread(edge, sizeof edge, 1, f) == 1 && edge[0] >= 0.0f &&
+             edge[0] < 1.0f && edge[1] > 0.0f;
+    }
     std::fclose(f);
     if (!ok) return sg_fail(s, FD2_ERR_IO, std::string("not a matching surrogate file: ") + path);
+    s->edge_amp = edge[0];
+    s->edge_len_um = edge[1];
     fd2_status st = fd2_sg_set_params(s, p.data(), (int64_t)p.size());
     if (st != FD2_OK) return st;
     s->norm_box = nb;

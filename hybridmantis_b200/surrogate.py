@@ -158,6 +158,60 @@ def radial_bin_probs(out: np.ndarray, bins: int = 96, radial_max_um: float = 400
     return (w[:, :, None] * M / S[:, :, None]).sum(1)
 
 
+def edge_weights(amplitude: float, length_um: float, x, y, det_x: float, det_y: float) -> np.ndarray:
+    """The sampler's azimuth acceptance at points (x, y) of a det_x x det_y
+    detector: prod over its four sides of (1 - amplitude exp(-s / length))."""
+    w = np.ones(np.broadcast(x, y).shape)
+    for s in (x, det_x - x, y, det_y - y):
+        w = w * (1.0 - amplitude * np.exp(-np.asarray(s, np.float64) / length_um))
+    return w
+
+
+def fit_edge(image, cx_um: float, cy_um: float, det_x: float, det_y: float, lb_x: float = 0.0, lb_y: float = 0.0,
+             pixel: float = 1.0):
+    """Fit the edge survival (amplitude, length) to a Monte Carlo PRF image
+    of depositions around (cx, cy): the image's own ring marginal (rings one
+    pixel wide around the centre), spread over each ring with the weights
+    edge_weights, is compared with the image on the rings at least half the
+    distance from the centre to the nearest side out (nearer in, the weights
+    are 1 and only the rings' discretisation would count); the pair with the
+    smallest L1 wins (amplitude 0 -- uniform rings -- included).  Returns
+    (amplitude, length_um, l1_uniform, l1_fitted) over those rings."""
+    img = np.asarray(image, np.float64)
+    img = img / img.sum()
+    nx, ny = img.shape
+    x = lb_x + (np.arange(nx) + 0.5) * pixel
+    y = lb_y + (np.arange(ny) + 0.5) * pixel
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    r = np.hypot(X - cx_um, Y - cy_um).ravel()
+    rb = np.floor(r / pixel).astype(np.int64)
+    ring = np.bincount(rb, img.ravel())
+    flat = img.ravel()
+    far = r >= 0.5 * min(cx_um, det_x - cx_um, cy_um, det_y - cy_um)
+
+    def l1(a, l):
+        w = edge_weights(a, l, X, Y, det_x, det_y).ravel() if a > 0 else np.ones_like(flat)
+        pred = ring[rb] * w / np.maximum(np.bincount(rb, w)[rb], 1e-300)
+        return float(np.abs(pred - flat)[far].sum())
+
+    base = l1(0.0, 1.0)
+    best = (base, 0.0, 1.0)
+    for a in np.arange(0.05, 0.95, 0.05):
+        for l in (5, 8, 12, 16, 20, 25, 30, 36, 43, 50, 60, 75, 90):
+            v = l1(a, l)
+            if v < best[0]:
+                best = (v, float(a), float(l))
+    if best[1] > 0:
+        # local refinement around the grid's best point
+        _, a0, l0 = best
+        for a in np.linspace(max(a0 - 0.05, 0.01), min(a0 + 0.05, 0.95), 11):
+            for l in np.linspace(0.8 * l0, 1.2 * l0, 9):
+                v = l1(a, l)
+                if v < best[0]:
+                    best = (v, float(a), float(l))
+    return best[1], best[2], base, best[0]
+
+
 class Surrogate:
     """One surrogate network with its optimizer state on a GPU."""
 
@@ -239,6 +293,15 @@ class Surrogate:
         h.lo[:] = [float(v) for v in lo]
         h.hi[:] = [float(v) for v in hi]
         self._check(self._lib.fd2_sg_set_hull(self._h, ctypes.byref(h)), "set_hull")
+
+    def set_edge(self, amplitude: float, length_um: float):
+        """Edge survival of the in-loop sampler's azimuths (see fit_edge)."""
+        self._check(self._lib.fd2_sg_set_edge(self._h, float(amplitude), float(length_um)), "set_edge")
+
+    def edge(self):
+        a, l = ctypes.c_float(), ctypes.c_float()
+        self._check(self._lib.fd2_sg_get_edge(self._h, ctypes.byref(a), ctypes.byref(l)), "get_edge")
+        return float(a.value), float(l.value)
 
     def save(self, path: str):
         self._check(self._lib.fd2_sg_save(self._h, path.encode()), "save")

@@ -13,6 +13,11 @@ a cosine step-size decay, batch 8,192, 5 % held out.
 detector of one benchmark configuration only (the detector a simulation
 campaign uses), with the routing hull narrowed to it.
 
+``--edge-config CONFIG`` fits the in-loop sampler's edge survival
+(surrogate.fit_edge) to a Monte Carlo PRF image of ``--edge-xrays`` x-rays of
+that configuration and saves it with the network; with ``--steps 0`` and
+``--init`` only that fit is made.
+
 Prints one JSON line with the losses and timings; writes the network with
 ``--out``.
 """
@@ -25,6 +30,25 @@ import numpy as np
 
 from . import fastdetect2 as fd
 from . import surrogate as sgm
+
+
+def fit_edge_from_mc(s, config: int, xrays: int, seed: int, device: int):
+    """Fit and set the surrogate's edge survival from a Monte Carlo PRF image
+    of `xrays` x-rays of `config` (no fit for config < 0)."""
+    if config < 0:
+        return None
+    es = fd.synth_events(config, xrays, seed + 7)
+    with fd.OpticalTransport(es.params, device=device, seed=seed + 8) as t:
+        t.submit(es)
+        t.run_sync()
+        img = t.prf()
+    p = es.params
+    amp, length, l1_uniform, l1_fit = sgm.fit_edge(img, float(np.mean(es.x_um)), float(np.mean(es.y_um)), p.det_x,
+                                                   p.det_y, p.lb_x, p.lb_y, p.pixel)
+    if amp > 0:
+        s.set_edge(amp, length)
+    return {"config": config, "xrays": xrays, "amplitude": amp, "length_um": length, "ring_l1_uniform": l1_uniform,
+            "ring_l1_fitted": l1_fit}
 
 
 def main():
@@ -44,7 +68,17 @@ def main():
     ap.add_argument("--radial-weight", type=float, default=1.0,
                     help="weight of the radial cross-entropy against the detection BCE in the loss")
     ap.add_argument("--out", default="")
+    ap.add_argument("--edge-config", type=int, default=-1)
+    ap.add_argument("--edge-xrays", type=int, default=200_000)
     a = ap.parse_args()
+    if a.steps == 0 and a.init:
+        with sgm.Surrogate(device=a.device) as s:
+            s.load(a.init)
+            edge = fit_edge_from_mc(s, a.edge_config, a.edge_xrays, a.seed, a.device)
+            if a.out:
+                s.save(a.out)
+        print(json.dumps({"edge": edge}))
+        return
     t0 = time.perf_counter()
     if a.focus >= 0:
         geoms = [fd.params_to_geometry(fd.synth_events(a.focus, 1, 1).params)]
@@ -74,12 +108,13 @@ def main():
             curve.append({"step": done, "train": tl, "val": vl})
         t_train = time.perf_counter() - t1
         after = s.eval()
+        edge = fit_edge_from_mc(s, a.edge_config, a.edge_xrays, a.seed, a.device)
         if a.out:
             s.save(a.out)
     print(json.dumps({"points": len(f), "photons_per_point": a.photons, "geometries": a.geometries,
                       "label_s": t_label, "label_photons_per_s": float(np.sum(ph)) / t_label,
                       "train_s": t_train, "steps": a.steps, "batch": a.batch,
-                      "val_before": before, "val_after": after, "curve": curve}))
+                      "val_before": before, "val_after": after, "curve": curve, "edge": edge}))
 
 
 if __name__ == "__main__":

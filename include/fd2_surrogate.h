@@ -118,6 +118,15 @@ FD2_API fd2_status fd2_sg_get_hull(fd2_sg *sg, fd2_sg_hull *hull);
 FD2_API fd2_status fd2_sg_set_hull(fd2_sg *sg, const fd2_sg_hull *hull);
 FD2_API fd2_status fd2_sg_save(fd2_sg *sg, const char *path);
 FD2_API fd2_status fd2_sg_load(fd2_sg *sg, const char *path);
+/* Edge survival of the sampled azimuths in fd2_sg_run: a detected photon's
+ * azimuth (its radius drawn from the network) is accepted with probability
+ * prod over the detector's four sides (1 - amplitude exp(-s / length_um)),
+ * s its distance to the side, redrawn otherwise; amplitude 0 (the default)
+ * = uniform over the directions that stay on the detector.  Fitted per model
+ * from a Monte Carlo PRF image of its geometry (surrogate.fit_edge) and
+ * saved with the network.  0 <= amplitude < 1, length_um > 0. */
+FD2_API fd2_status fd2_sg_set_edge(fd2_sg *sg, float amplitude, float length_um);
+FD2_API fd2_status fd2_sg_get_edge(const fd2_sg *sg, float *amplitude, float *length_um);
 
 /* One forward and backward pass on the given batch (host arrays, b rows,
  * b <= batch): loss and the gradient of every parameter (same order as

@@ -91,3 +91,35 @@ def test_out_of_hull_events_use_monte_carlo(trained):
     assert sr["stats"]["surrogate_events"] == 0
     assert np.array_equal(sr["prim"], mc["prim"])
     assert np.array_equal(sr["prf"], mc["prf"])
+
+
+def test_edge_survival_moves_positions_only(trained, tmp_path):
+    """The sampler's edge survival redraws azimuths only: per-history counts,
+    counters and the radial profile's first rings are those of the run
+    without it, while light near the detector's sides thins out; the
+    setting travels with the saved network."""
+    sg, es = trained
+    assert sg.edge() == (0.0, 1.0)
+    plain = _run(es, sg, audit=0.0)
+    sg.set_edge(0.5, 40.0)
+    try:
+        edged = _run(es, sg, audit=0.0)
+        path = str(tmp_path / "edge.fd2sg")
+        sg.save(path)
+        with sgm.Surrogate(hidden=256, batch=2048) as s2:
+            s2.load(path)
+            assert s2.edge() == (0.5, 40.0)
+    finally:
+        sg.set_edge(0.0, 1.0)
+    assert np.array_equal(plain["prim"], edged["prim"])
+    assert plain["counters"]["detected"] == edged["counters"]["detected"]
+    assert not np.array_equal(plain["prf"], edged["prf"])
+    # the same light within the image, less of it along the sides
+    a, b = plain["prf"].astype(np.float64), edged["prf"].astype(np.float64)
+    assert abs(a.sum() - b.sum()) <= 1e-3 * a.sum()
+    side = np.zeros(a.shape, bool)
+    side[:20, :] = side[-20:, :] = side[:, :20] = side[:, -20:] = True
+    assert b[side].sum() < a[side].sum()
+    for bad in ((1.0, 10.0), (-0.1, 10.0), (0.5, 0.0)):
+        with pytest.raises(Exception):
+            sg.set_edge(*bad)

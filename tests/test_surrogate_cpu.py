@@ -7,6 +7,7 @@ compares against formulas that are themselves verified.
 import numpy as np
 
 from oracle import sg_oracle as so
+from hybridmantis_b200 import surrogate as sgm
 
 
 def _problem(seed, n=24, hidden=64):
@@ -69,3 +70,31 @@ def test_bf16_rounding():
     assert r[3] == 1.0 + 2 ** -7                   # above half an ulp
     assert r[4] == -2.5
     assert abs(r[5] - 3.0e-20) / 3.0e-20 < 2 ** -8
+
+
+def test_fit_edge_recovers_the_edge_survival():
+    """fit_edge explains an image whose rings are spread with the sampler's
+    edge weights as well as the true weights do (amplitude and length trade
+    off against each other in part, so the pair itself is not unique), and
+    finds nothing to explain in uniform rings."""
+    n, c = 301, 150.5
+    x = np.arange(n) + 0.5
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    profile = np.exp(-np.hypot(X - c, Y - c) / 60.0)
+    for amp, length in ((0.5, 30.0), (0.3, 12.0)):
+        img = profile * sgm.edge_weights(amp, length, X, Y, float(n), float(n))
+        fa, fl, l1u, l1f = sgm.fit_edge(img, c, c, float(n), float(n))
+        assert fa > 0.0, (fa, fl)
+        # the true pair's residual: the rings' own discretisation
+        w = sgm.edge_weights(fa, fl, X, Y, float(n), float(n))
+        assert l1f < 0.25 * l1u, (fa, fl, l1u, l1f)
+        # the fitted weights reproduce the side-to-corner contrast of the image
+        r = np.hypot(X - c, Y - c)
+        band = (r > 120) & (r < 145)
+        towards_side = band & (np.minimum(np.abs(X - c), np.abs(Y - c)) < 20)
+        towards_corner = band & (np.abs(np.abs(X - c) - np.abs(Y - c)) < 20)
+        truth = img[towards_side].mean() / img[towards_corner].mean()
+        fitted = (profile * w)[towards_side].mean() / (profile * w)[towards_corner].mean()
+        assert abs(fitted - truth) <= 0.02 * truth, (fa, fl, truth, fitted)
+    fa, fl, l1u, l1f = sgm.fit_edge(profile, c, c, float(n), float(n))
+    assert fa == 0.0 or l1f > 0.8 * l1u, (fa, fl, l1u, l1f)
