@@ -376,13 +376,18 @@ void fit_window(fd2_ctx *c)
 // at 64 registers; 6.7e8 photons/s against 5.8e8 for 320 x 2), chunks of 16
 // photons; several geometries 256 x 3 (8.5e8 against 7.9e8 for 256 x 4,
 // whose variant spills); the column lattice 320 x 2 (2.2e8 against 2.0e8 for
-// 256 x 2 or x 3); label mode 256 x 2 (its only variant).
+// 256 x 2 or x 3); label mode with one geometry (the surrogate's audit) as
+// one geometry, with several 256 x 2.
 static void default_launch(const fd2_ctx *c, int n_geom, fd2::TransportConfig *cfg)
 {
     int block = 256, ctas = 4, chunk = 16;
     if (c->opt.radial_bins > 0) {
-        ctas = 2;
-        chunk = 32;
+        // label mode: one geometry (the surrogate's audit) as a production
+        // run; several (training labels) 256 x 2
+        if (n_geom > 1) {
+            ctas = 2;
+            chunk = 32;
+        }
     } else if (c->opt.column_grid) {
         block = 320;
         ctas = 2;

@@ -724,7 +724,7 @@ cudaError_t launch_fill_chunks(cudaStream_t s, int64_t n, int chunk, const int32
     X(true, 256, 4, false, false, false) X(false, 256, 3, false, true, false)              \
     X(false, 512, 1, false, false, true) X(false, 256, 2, false, false, true)              \
     X(false, 320, 2, false, false, true) X(false, 256, 3, false, false, true)              \
-    X(false, 256, 4, false, false, true)
+    X(false, 256, 4, false, false, true) X(false, 256, 4, true, false, false)
 
 cudaError_t prepare_transport(const TransportConfig &cfg, int n_geom)
 {
@@ -771,9 +771,14 @@ cudaError_t launch_transport(cudaStream_t s, const TransportConfig &cfg, int sm_
         else if (cfg.block <= 256) transport_kernel<false, 256, 2, false, true><<<grid, cfg.block, smem, s>>>(a);
         else return cudaErrorInvalidConfiguration;
     } else if (a.radial) {
-        // label mode: one variant, 256 threads, two CTAs per SM
+        // label mode, 256 threads: one geometry (the surrogate's audit) as the
+        // production kernel, four CTAs per SM; several geometries (training
+        // labels) two CTAs per SM
         if (cfg.block > 256) return cudaErrorInvalidConfiguration;
-        transport_kernel<true, 256, 2, true><<<(unsigned)(sm_count * 2), cfg.block, smem, s>>>(a);
+        if (!multi && cfg.ctas_per_sm >= 4)
+            transport_kernel<false, 256, 4, true><<<(unsigned)(sm_count * 4), cfg.block, smem, s>>>(a);
+        else
+            transport_kernel<true, 256, 2, true><<<(unsigned)(sm_count * 2), cfg.block, smem, s>>>(a);
     } else if (!multi && cfg.aggregate) {
         // warp-aggregated, shared-memory privatised tallies (tally_mode 1)
         if (cfg.block == 320) transport_kernel<false, 320, 2, false, false, true><<<grid, cfg.block, smem, s>>>(a);

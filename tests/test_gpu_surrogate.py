@@ -83,6 +83,23 @@ def test_label_mode_counts_every_detected_photon(require_gpu):
         assert np.array_equal(t.detected_per_primary(), det)
 
 
+def test_label_mode_single_geometry_counts_every_detected_photon(require_gpu):
+    """Label mode with one geometry (the surrogate's audit runs it) uses the
+    single-geometry kernel shape: its per-history counts equal a production
+    run of the same photons, and its radial bins hold every detection."""
+    g = sgm.sample_geometries(1, seed=15)[0]
+    f, ph, det, rad = sgm.label_points([g], 96, 1500, seed=19, lateral_um=0.0)
+    assert np.array_equal(det, rad.sum(1).astype(np.int32))
+    p = hb.default_params(num_hist=96)
+    with hb.OpticalTransport(p, count_mode=hb.COUNT_GIVEN, seed=19) as t:
+        t.set_geometries([g])
+        n = len(f)
+        t.submit_events_um(np.full(n, g.det_x / 2), np.full(n, g.det_y / 2), g.det_height / 2 - f[:, 0],
+                           f[:, 1] * 1000, np.arange(1, n + 1), nphot=ph, geom=np.zeros(n, np.uint16))
+        t.run_sync()
+        assert np.array_equal(t.detected_per_primary(), det)
+
+
 def _constant_predictor_losses(t_tr, y_tr, t_va, y_va):
     pc = np.clip(t_tr.mean(), 1e-6, 1 - 1e-6)
     det = -(t_va * np.log(pc) + (1 - t_va) * np.log(1 - pc)).mean()
