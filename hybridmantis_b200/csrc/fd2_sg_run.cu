@@ -176,6 +176,7 @@ struct SampleArgs {
     float edge_amp, edge_inv_len;  // edge survival of the azimuths (amplitude 0: off)
 };
 
+constexpr int kSampleThreads = 256;  // one warp per event
 constexpr uint32_t kDomainRetry = 0x52455452u;  // rejection retries of ring_radius
 constexpr uint32_t kDomainTurn = 0x5455524eu;   // azimuth retries
 
@@ -203,9 +204,11 @@ __device__ __forceinline__ float ring_radius(float mu, float sd, float S, float 
 }
 
 // Detected photons of one row and their PRF pixels; one warp per row.
-__global__ void sample_kernel(const SampleArgs a)
+__global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs a)
 {
     const int lane = threadIdx.x & 31;
+    __shared__ float s_mix[kSampleThreads / 32][4][kComponents];
+    float(*mix)[kComponents] = s_mix[threadIdx.x >> 5];
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int rows = *a.count;
     const uint32_t run = *a.run_tag;
@@ -271,26 +274,35 @@ __global__ void sample_kernel(const SampleArgs a)
         // s the point's distance to the side: the detected light thins out
         // towards the detector's sides, whose crossing loses a photon.  Only
         // the azimuth is redrawn, so the radius keeps the network's law.
-        Mix m;
-        decode_mix(o, m);
-        float cumw[kComponents];
+        // the event's mixture in the warp's shared-memory table (every lane
+        // draws from the same one; an indexed table in registers would go to
+        // local memory): cumulative weight, mu, sd and normaliser per ring
         {
+            Mix m;
+            decode_mix(o, m);
             float acc = 0.0f;
+            __syncwarp();  // the previous event's photons are placed
 #pragma unroll
             for (int c = 0; c < kComponents; ++c) {
                 acc += m.w[c];
-                cumw[c] = acc;
+                if (lane == c) {
+                    mix[0][c] = c == kComponents - 1 ? 2.0f : acc;
+                    mix[1][c] = m.mu[c];
+                    mix[2][c] = m.sd[c];
+                    mix[3][c] = m.S[c];
+                }
             }
-            cumw[kComponents - 1] = 2.0f;
+            __syncwarp();
         }
         int32_t in_prf = 0;
         for (int32_t i = lane; i < total; i += 32) {
             const uint4 h = philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainPlace, run),
                                      a.k0, a.k1);
+            // the component: the first whose cumulative weight exceeds u
             const float u = unit(h.x);
             int c = 0;
-            while (c < kComponents - 1 && u >= cumw[c]) ++c;
-            const float rad = ring_radius(m.mu[c], m.sd[c], m.S[c], unit(h.y), unit(h.w), (uint32_t)i, ge, run,
+            while (c < kComponents - 1 && u >= mix[0][c]) ++c;
+            const float rad = ring_radius(mix[1][c], mix[2][c], mix[3][c], unit(h.y), unit(h.w), (uint32_t)i, ge, run,
                                           a.k0, a.k1);
             float sn, cs;
             sincospif(2.0f * unit(h.z), &sn, &cs);
@@ -485,7 +497,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
         a.run_tag = reinterpret_cast<const uint32_t *>(c->d_flags + 1);
         a.edge_amp = s->edge_amp;
         a.edge_inv_len = 1.0f / s->edge_len_um;
-        sample_kernel<<<(unsigned)(c->sm_count * 8), 256, 0, q>>>(a);
+        sample_kernel<<<(unsigned)(c->sm_count * 8), kSampleThreads, 0, q>>>(a);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaEventRecord(R->ev[3], q);
