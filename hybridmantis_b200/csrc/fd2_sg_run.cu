@@ -95,8 +95,6 @@ __device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1)
 __device__ __forceinline__ float unit(uint32_t r) { return ((float)(r >> 8) + 0.5f) * 5.9604644775390625e-8f; }
 
 constexpr uint32_t kDomainAudit = 0x41554449u;   // audit selection
-constexpr uint32_t kDomainBinom = 0x42494e4fu;   // detected counts
-constexpr uint32_t kDomainPlace = 0x504c4143u;   // photon positions
 
 struct RouteArgs {
     int64_t n;
@@ -177,8 +175,33 @@ struct SampleArgs {
 };
 
 constexpr int kSampleThreads = 256;  // one warp per event
-constexpr uint32_t kDomainRetry = 0x52455452u;  // rejection retries of ring_radius
-constexpr uint32_t kDomainTurn = 0x5455524eu;   // azimuth retries
+constexpr uint32_t kDomainLane = 0x4c414e45u;   // a lane's stream for one event
+
+// A lane's random stream for one event (its detected count and its photons'
+// places): xoshiro128+ (Blackman & Vigna, ACM TOMS 47(4), 2021) seeded by one
+// Philox-4x32-10 block at (lane, event, domain, run), the construction of the
+// transport's per-photon streams; floats from the top 24 bits (unit()).  A
+// lane takes photons lane, lane + 32, ... of its event in order, so every
+// draw is fixed by the event, the lane and the run.
+struct LaneRng {
+    uint32_t s0, s1, s2, s3;
+    __device__ __forceinline__ LaneRng(uint4 k)
+        : s0(k.x), s1(k.y), s2(k.z), s3(k.w | ((k.x | k.y | k.z | k.w) == 0u ? 1u : 0u))
+    {
+    }
+    __device__ __forceinline__ float u()
+    {
+        const uint32_t r = s0 + s3;
+        const uint32_t t = s1 << 9;
+        s2 ^= s0;
+        s3 ^= s1;
+        s1 ^= s2;
+        s0 ^= s3;
+        s2 ^= t;
+        s3 = __funnelshift_l(s3, s3, 11);
+        return unit(r);
+    }
+};
 
 // Radius from one ring component, density proportional to r N(r; mu, sd) on
 // r >= 0, exactly.  In t = (r - mu) / sd the weight (mu + sd t) phi(t) splits
@@ -186,9 +209,8 @@ constexpr uint32_t kDomainTurn = 0x5455524eu;   // azimuth retries
 // sd phi(0), a Rayleigh), and t0 <= t < 0, t0 = -mu / sd: a normal on
 // [t0, 0) thinned with acceptance 1 + sd t / mu (mass S - mu / 2 - sd phi(0),
 // at least half of its proposals accepted).  u picks the region, v is the
-// region's uniform; rejections draw fresh uniforms.
-__device__ __forceinline__ float ring_radius(float mu, float sd, float S, float u, float v, uint32_t i, uint64_t ge,
-                                             uint32_t run, uint32_t k0, uint32_t k1)
+// region's uniform; rejections draw fresh uniforms from `rng`.
+__device__ __forceinline__ float ring_radius(float mu, float sd, float S, float u, float v, LaneRng &rng)
 {
     const float m1 = 0.5f * mu, m2 = sd * 0.3989422804014327f;
     const float x = u * S;
@@ -196,9 +218,8 @@ __device__ __forceinline__ float ring_radius(float mu, float sd, float S, float 
     if (x < m1 + m2 || mu <= 0.0f) return mu + sd * sqrtf(-2.0f * logf(v));
     const float t0 = -mu / sd, c0 = normcdff(t0), span = 0.5f - c0;
     for (uint32_t k = 0; k < 64; ++k) {
-        const uint4 h = philox10(make_uint4(i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainRetry, run * 64u + k), k0, k1);
-        const float t = fminf(normcdfinvf(fmaxf(c0 + unit(h.x) * span, 1e-37f)), 0.0f);
-        if (unit(h.y) <= 1.0f + sd * t / mu) return fmaxf(mu + sd * t, 0.0f);
+        const float t = fminf(normcdfinvf(fmaxf(c0 + rng.u() * span, 1e-37f)), 0.0f);
+        if (rng.u() <= 1.0f + sd * t / mu) return fmaxf(mu + sd * t, 0.0f);
     }
     return 0.5f * mu;  // not reached in practice (acceptance >= 1/2 per proposal)
 }
@@ -220,6 +241,8 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
         const fd2::DevGeom &g = a.geoms[gi];
         const float4 pos = a.ev_pos[e];
         const uint64_t ge = (uint64_t)(a.event_base + e);
+        LaneRng rng(philox10(make_uint4((uint32_t)lane, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainLane, run), a.k0,
+                             a.k1));
         // ---- detected count: lane l takes photons [lo, hi) of the N
         const float z = o[0];
         const float p = 1.0f / (1.0f + expf(-z));
@@ -235,25 +258,12 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
                 const float q = flip ? 1.0f - p : p;
                 const float inv_log = 1.0f / log1pf(-q);
                 int32_t hits = 0, at = -1;
-                uint32_t ctr = 0;
                 for (;;) {
-                    const uint4 h = philox10(make_uint4(ctr++, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainBinom,
-                                                        run * 32u + (uint32_t)lane),
-                                             a.k0, a.k1);
-                    const uint32_t w4[4] = {h.x, h.y, h.z, h.w};
-                    bool done = false;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float skip = floorf(logf(unit(w4[j])) * inv_log);
-                        const float next = (float)at + skip + 1.0f;
-                        if (next >= (float)span) {
-                            done = true;
-                            break;
-                        }
-                        at = (int32_t)next;
-                        ++hits;
-                    }
-                    if (done) break;
+                    const float skip = floorf(logf(rng.u()) * inv_log);
+                    const float next = (float)at + skip + 1.0f;
+                    if (next >= (float)span) break;
+                    at = (int32_t)next;
+                    ++hits;
                 }
                 k = flip ? span - hits : hits;
             }
@@ -296,34 +306,26 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
         }
         int32_t in_prf = 0;
         for (int32_t i = lane; i < total; i += 32) {
-            const uint4 h = philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainPlace, run),
-                                     a.k0, a.k1);
             // the component: the first whose cumulative weight exceeds u
-            const float u = unit(h.x);
+            const float u = rng.u();
             int c = 0;
             while (c < kComponents - 1 && u >= mix[0][c]) ++c;
-            const float rad = ring_radius(mix[1][c], mix[2][c], mix[3][c], unit(h.y), unit(h.w), (uint32_t)i, ge, run,
-                                          a.k0, a.k1);
+            const float ur = rng.u(), vr = rng.u();
+            const float rad = ring_radius(mix[1][c], mix[2][c], mix[3][c], ur, vr, rng);
             float sn, cs;
-            sincospif(2.0f * unit(h.z), &sn, &cs);
+            sincospif(2.0f * rng.u(), &sn, &cs);
             for (uint32_t k = 0; k < 32; ++k) {
                 const float tx = pos.x + rad * cs, ty = pos.y + rad * sn;
                 bool ok = tx >= 0.0f && tx <= g.xdet && ty >= 0.0f && ty <= g.ydet;
-                // attempt k's acceptance uniform and attempt k + 1's azimuth
-                uint4 hk = make_uint4(0u, 0u, 0u, 0u);
-                const bool draw = !ok || a.edge_amp > 0.0f;
-                if (draw)
-                    hk = philox10(make_uint4((uint32_t)i, (uint32_t)ge, (uint32_t)(ge >> 32) ^ kDomainTurn, run * 32u + k),
-                                  a.k0, a.k1);
                 if (ok && a.edge_amp > 0.0f) {
                     const float W = (1.0f - a.edge_amp * __expf(-tx * a.edge_inv_len)) *
                                     (1.0f - a.edge_amp * __expf(-(g.xdet - tx) * a.edge_inv_len)) *
                                     (1.0f - a.edge_amp * __expf(-ty * a.edge_inv_len)) *
                                     (1.0f - a.edge_amp * __expf(-(g.ydet - ty) * a.edge_inv_len));
-                    ok = unit(hk.y) < W;
+                    ok = rng.u() < W;
                 }
                 if (ok) break;
-                sincospif(2.0f * unit(hk.x), &sn, &cs);
+                sincospif(2.0f * rng.u(), &sn, &cs);
             }
             const float x = pos.x + rad * cs, y = pos.y + rad * sn;
             if (x <= g.ub_x && y <= g.ub_y && x >= g.lb_x && y >= g.lb_y) {
