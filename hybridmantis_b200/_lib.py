@@ -113,7 +113,8 @@ class SgConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("hidden", ctypes.c_int32), ("radial_bins", ctypes.c_int32),
                 ("radial_max_um", ctypes.c_double), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
                 ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("adam_eps", ctypes.c_float),
-                ("radial_weight", ctypes.c_float), ("lateral_um", ctypes.c_float), ("seed", ctypes.c_uint64)]
+                ("radial_weight", ctypes.c_float), ("lateral_um", ctypes.c_float), ("seed", ctypes.c_uint64),
+                ("depth_margin_um", ctypes.c_float)]
 
 
 class SgHull(ctypes.Structure):

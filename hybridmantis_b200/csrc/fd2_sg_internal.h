@@ -53,6 +53,7 @@ struct fd2_sg {
     double radial_max = 200.0;
     float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f, lambda = 1.0f;
     float lateral_um = 50.0f;
+    float depth_margin_um = 1.0f;  // depths this far outside the hull take its edge
     // edge survival of the sampled azimuths (fd2_sg_set_edge): amplitude and
     // length; amplitude 0 = uniform over the directions that stay on the detector
     float edge_amp = 0.0f, edge_len_um = 1.0f;

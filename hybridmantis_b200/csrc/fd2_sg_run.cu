@@ -107,6 +107,7 @@ struct RouteArgs {
     NormParams norm;
     fd2_sg_hull hull;
     float lateral;  // largest |x - centre|, |y - centre| a surrogate row may have
+    float depth_margin;  // depths this far outside the hull's range take its edge
     float audit_frac;
     uint32_t k0, k1;
     int64_t event_base;
@@ -131,6 +132,10 @@ __global__ void route_kernel(const RouteArgs a)
         f[5] = g.beta;
         f[6] = 1.0f - g.top_absfrac;
         f[7] = g.mu > 0.0f ? log10f(g.mu) : -INFINITY;
+        // a deposition just outside the labels' depth range (they leave out
+        // the layer's first and last 0.1 %) takes the range's edge depth
+        if (f[0] < a.hull.lo[0] && f[0] >= a.hull.lo[0] - a.depth_margin) f[0] = a.hull.lo[0];
+        if (f[0] > a.hull.hi[0] && f[0] <= a.hull.hi[0] + a.depth_margin) f[0] = a.hull.hi[0];
         bool in = fabsf(p.x - 0.5f * g.xdet) <= a.lateral && fabsf(p.y - 0.5f * g.ydet) <= a.lateral;
 #pragma unroll
         for (int i = 0; i < kFeatures; ++i) in = in && f[i] >= a.hull.lo[i] && f[i] <= a.hull.hi[i];
@@ -455,6 +460,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
             a.hull.hi[i] += tol;
         }
         a.lateral = s->lateral_um;
+        a.depth_margin = s->depth_margin_um;
         a.audit_frac = (float)audit_fraction;
         a.k0 = k0;
         a.k1 = k1;

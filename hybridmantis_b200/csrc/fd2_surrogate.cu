@@ -785,6 +785,7 @@ void fd2_sg_default_config(fd2_sg_config *c)
     c->radial_weight = 1.0f;
     c->lateral_um = 50.0f;
     c->seed = 0x5347fd2ull;
+    c->depth_margin_um = 1.0f;
 }
 
 const char *fd2_sg_last_error(const fd2_sg *s) { return s ? s->last_error.c_str() : "no surrogate"; }
@@ -798,7 +799,7 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     else fd2_sg_default_config(&c);
     if (c.hidden < 64 || c.hidden % 64 || c.hidden > 1024 || c.radial_bins < 1 || c.radial_bins > 1024 ||
         !(c.radial_max_um > 0) || c.batch < 64 || c.batch % 64 || c.batch > (1 << 20) || !(c.lr > 0) ||
-        !(c.lateral_um >= 0))
+        !(c.lateral_um >= 0) || !(c.depth_margin_um >= 0))
         return FD2_ERR_INVALID_ARGUMENT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return FD2_ERR_NO_DEVICE;
@@ -815,6 +816,7 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
     s->eps = c.adam_eps;
     s->lambda = c.radial_weight;
     s->lateral_um = c.lateral_um;
+    s->depth_margin_um = c.depth_margin_um;
     s->seed = c.seed;
     for (int i = 0; i < kFeatures; ++i) {
         s->hull.lo[i] = 0.0f;

@@ -217,13 +217,14 @@ class Surrogate:
 
     def __init__(self, device: int = 0, hidden: int = 256, radial_bins: int = 96, radial_max_um: float = 400.0,
                  batch: int = 8192, lr: float = 1e-3, radial_weight: float = 1.0, seed: int = 0x5347fd2,
-                 lateral_um: float = 50.0):
+                 lateral_um: float = 50.0, depth_margin_um: float = 1.0):
         lib = load()
         self._lib = lib
         c = SgConfig()
         lib.fd2_sg_default_config(ctypes.byref(c))
         c.device, c.hidden, c.radial_bins, c.radial_max_um = device, hidden, radial_bins, radial_max_um
         c.batch, c.lr, c.radial_weight, c.seed, c.lateral_um = batch, lr, radial_weight, seed, lateral_um
+        c.depth_margin_um = depth_margin_um
         self.config = c
         self.radial_bins = radial_bins
         self.radial_max_um = radial_max_um

@@ -65,6 +65,10 @@ typedef struct fd2_sg_config {
                                 the labels sit at the centre, so their far light is
                                 what the detector's edges leave from there; 50 */
     uint64_t seed;           /* initialisation and batch sampling */
+    float depth_margin_um;   /* fd2_sg_run: a deposition at most this far outside the
+                                hull's depth range (the labels leave out the first and
+                                last 0.1 % of the layer) is given the range's edge
+                                depth and goes to the network; 1 */
 } fd2_sg_config;
 
 /* Box of the training data: events whose features lie outside it go to the

@@ -123,3 +123,23 @@ def test_edge_survival_moves_positions_only(trained, tmp_path):
     for bad in ((1.0, 10.0), (-0.1, 10.0), (0.5, 0.0)):
         with pytest.raises(Exception):
             sg.set_edge(*bad)
+
+
+def test_depth_margin_routes_depositions_just_outside_the_labels(trained, tmp_path):
+    """Depositions a fraction of a micrometre shallower than the hull's depth
+    range go to the network with the default 1-um margin (at the range's
+    edge depth) and to the Monte Carlo without it."""
+    sg, es = trained
+    lo, _ = sg.hull()
+    assert 0.0 < lo[0] < 1.0
+    moved = es.subset(np.arange(es.n))
+    moved.z_um = np.full(es.n, es.params.det_height / 2 - 0.5 * lo[0], np.float32)
+    with_margin = _run(moved, sg, audit=0.0)["stats"]
+    path = str(tmp_path / "net.fd2sg")
+    sg.save(path)
+    with sgm.Surrogate(hidden=256, batch=2048, depth_margin_um=0.0) as s0:
+        s0.load(path)
+        without = _run(moved, s0, audit=0.0)["stats"]
+    n_with = with_margin["surrogate_events"] + with_margin["mc_events"]
+    assert with_margin["surrogate_events"] >= 0.9 * n_with
+    assert without["surrogate_events"] == 0 and without["mc_events"] == n_with
