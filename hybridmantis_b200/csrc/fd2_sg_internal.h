@@ -99,6 +99,7 @@ struct fd2_sg {
     // tile whose completion wait gave up sets the fault word
     bool use_tc = true;
     bool tc_pipe = true;  // the pipelined tcgen05 kernel (FD2_SG_GEMM=tc1: the one-tile-at-a-time kernel)
+    bool tc_tma = true;   // its operands by TMA where possible (FD2_SG_GEMM=cpasync: cp.async)
     unsigned *d_tc_fault = nullptr;
     int sm_count = 148;
 };

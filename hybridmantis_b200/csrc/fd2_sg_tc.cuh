@@ -35,6 +35,7 @@
 // with 16-byte cp.async copies from this GPU's memory.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -62,6 +63,11 @@ struct TcArgs {
     int ldc;
     long long a_split, b_split, c_split;  // element offsets of slice blockIdx.y
     unsigned *fault;  // set when a wait gives up (the tile is then not stored)
+    // pipelined kernel: stage A and B with TMA (no slices) through these maps
+    // of A (K x M rows) and B (K x N rows), boxes of 8 K-elements (one 16-byte
+    // column of the canonical layout) by 128 rows (A) or N rows (B)
+    int tma;
+    CUtensorMap tmap_a, tmap_b;
 };
 
 // Dynamic shared memory of one CTA: A tile + B.
@@ -351,6 +357,22 @@ __device__ __forceinline__ void tc_mbar_arrive(uint32_t bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// TMA: one 2D box into shared memory, completing on `bar` by its bytes.
+__device__ __forceinline__ void tc_tma_load(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// Arrive on `bar` and add `bytes` to the transfers its phase waits for.
+__device__ __forceinline__ void tc_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void tc_commit(uint32_t bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -377,11 +399,11 @@ __device__ __forceinline__ void tc_stage_chunk(unsigned char *dst, const __nv_bf
 }
 
 template <int kEpi>
-__global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcArgs g)
+__global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __grid_constant__ TcArgs g)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ __align__(8) unsigned long long s_full[kPipeStages], s_empty[kPipeStages], s_accf[2], s_acce[2],
-        s_drain;
+        s_drain, s_bfull;
     __shared__ uint32_t s_taddr;
     __shared__ int s_fault;
     __shared__ __align__(16) float s_bias[kTcMaxN];
@@ -413,9 +435,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
     const uint32_t accf0 = (uint32_t)__cvta_generic_to_shared(&s_accf[0]);
     const uint32_t acce0 = (uint32_t)__cvta_generic_to_shared(&s_acce[0]);
     const uint32_t drain = (uint32_t)__cvta_generic_to_shared(&s_drain);
+    const uint32_t bfull = (uint32_t)__cvta_generic_to_shared(&s_bfull);
+    const bool tma = g.tma != 0;
     if (threadIdx.x == 0) {
         for (int i = 0; i < kPipeStages; ++i) {
-            tc_mbar_init(full0 + 8u * i, 32 * kPipeProducers);  // the producer lanes
+            // the producer lanes, or (TMA) one arrive with the stage's bytes
+            tc_mbar_init(full0 + 8u * i, tma ? 1 : 32 * kPipeProducers);
             tc_mbar_init(empty0 + 8u * i, 1);  // one tcgen05.commit
         }
         for (int i = 0; i < 2; ++i) {
@@ -423,10 +448,19 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
             tc_mbar_init(acce0 + 8u * i, 4);   // one arrive per epilogue warp
         }
         tc_mbar_init(drain, 1);
+        tc_mbar_init(bfull, 1);
         s_fault = 0;
+        if (tma) {
+            // B (resident for all of the CTA's tiles) by TMA, one 16-byte K
+            // column of all N rows per box; only the MMA thread waits for it
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tc_expect_tx(bfull, (uint32_t)(N * K * 2));
+            const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
+            for (int c = 0; c < K / 8; ++c) tc_tma_load(b0 + (uint32_t)(c * N * 16), &g.tmap_b, c * 8, 0, bfull);
+        }
     }
     // B stays resident for all of the CTA's tiles
-    tc_stage_part(sB, gB, g.ldb, N, N, K, threadIdx.x, blockDim.x);
+    if (!tma) tc_stage_part(sB, gB, g.ldb, N, N, K, threadIdx.x, blockDim.x);
     for (int i = threadIdx.x; i < N; i += blockDim.x) s_bias[i] = kBias ? g.bias[i] : 0.0f;
     asm volatile("cp.async.wait_all;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -435,7 +469,34 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = s_taddr;
 
-    if (warp >= 4 && warp < kPipeMmaWarp) {
+    if (tma && warp >= 4 && warp < kPipeMmaWarp) {
+        // ---- producer (TMA): one thread; per chunk, once its stage is free,
+        // the stage's byte count on its `full` barrier and one box per 16-byte
+        // K column (rows past M arrive as zeros)
+        if (warp == 4 && lane == 0) {
+            int gc = 0;
+            bool ok = true;
+            const uint32_t r0 = (uint32_t)__cvta_generic_to_shared(sRing);
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+                const int m0 = tile * kTcRows;
+                for (int c = 0; c < nck; ++c, ++gc) {
+                    const int st = gc % kPipeStages;
+                    const uint32_t ph = (uint32_t)((gc / kPipeStages) & 1);
+                    if (!tc_wait(empty0 + 8u * st, ph ^ 1u)) {
+                        ok = false;
+                        s_fault = 1;
+                        if (g.fault) atomicOr(g.fault, 1u);
+                        break;
+                    }
+                    const uint32_t dst = r0 + (uint32_t)st * stage_bytes;
+                    tc_expect_tx(full0 + 8u * st, stage_bytes);
+                    for (int j = 0; j < CK / 8; ++j)
+                        tc_tma_load(dst + (uint32_t)(j * kTcRows * 16), &g.tmap_a, c * CK + j * 8, m0, full0 + 8u * st);
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp >= 4 && warp < kPipeMmaWarp) {
         // ---- producers: up to kPipeDepth chunks' copies in flight per lane
         // (cp.async groups); a chunk's stage is marked full once its group
         // has completed and a proxy fence has made the writes visible to the
@@ -481,6 +542,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const TcA
             const uint32_t r0 = (uint32_t)__cvta_generic_to_shared(sRing);
             int gc = 0, it = 0;
             bool ok = true;
+            if (tma && !tc_wait(bfull, 0u)) ok = false;  // B by TMA
             for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++it) {
                 const int a = it & 1;
                 if (!tc_wait(acce0 + 8u * a, (uint32_t)((it >> 1) & 1) ^ 1u)) {
