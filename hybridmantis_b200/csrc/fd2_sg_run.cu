@@ -212,21 +212,26 @@ struct LaneRng {
 // r >= 0, exactly.  In t = (r - mu) / sd the weight (mu + sd t) phi(t) splits
 // into t >= 0: mu phi(t) (mass mu / 2, a half-normal) and sd t phi(t) (mass
 // sd phi(0), a Rayleigh), and t0 <= t < 0, t0 = -mu / sd: a normal on
-// [t0, 0) thinned with acceptance 1 + sd t / mu (mass S - mu / 2 - sd phi(0),
-// at least half of its proposals accepted).  u picks the region, v is the
-// region's uniform; rejections draw fresh uniforms from `rng`.
-__device__ __forceinline__ float ring_radius(float mu, float sd, float S, float u, float v, LaneRng &rng)
+// [t0, 0) thinned with acceptance 1 + sd t / mu (mass S - mu / 2 - sd phi(0)).
+// u picks the region.  All three come from one Box-Muller pair: rho =
+// sqrt(-2 ln u1) is the Rayleigh, rho |cos(2 pi u2)| the half-normal, and its
+// negative, kept when it is >= t0 and passes the thinning, the third region
+// (retried with fresh draws otherwise), so the regions share their costly part.
+__device__ __forceinline__ float ring_radius(float mu, float sd, float S, float u, LaneRng &rng)
 {
     const float m1 = 0.5f * mu, m2 = sd * 0.3989422804014327f;
     const float x = u * S;
-    if (x < m1) return mu + sd * normcdfinvf(0.5f + 0.5f * fminf(v, 1.0f - 6e-8f));
-    if (x < m1 + m2 || mu <= 0.0f) return mu + sd * sqrtf(-2.0f * logf(v));
-    const float t0 = -mu / sd, c0 = normcdff(t0), span = 0.5f - c0;
+    const bool rayleigh = x >= m1 && (x < m1 + m2 || mu <= 0.0f);
+    const bool upper = x < m1;
+    const float t0 = -mu / sd;
     for (uint32_t k = 0; k < 64; ++k) {
-        const float t = fminf(normcdfinvf(fmaxf(c0 + rng.u() * span, 1e-37f)), 0.0f);
-        if (rng.u() <= 1.0f + sd * t / mu) return fmaxf(mu + sd * t, 0.0f);
+        const float rho = sqrtf(-2.0f * logf(rng.u()));
+        if (rayleigh) return mu + sd * rho;
+        const float z = rho * fabsf(__cosf(6.283185307179586f * rng.u()));
+        if (upper) return mu + sd * z;
+        if (-z >= t0 && rng.u() <= 1.0f - sd * z / mu) return fmaxf(mu - sd * z, 0.0f);
     }
-    return 0.5f * mu;  // not reached in practice (acceptance >= 1/2 per proposal)
+    return 0.5f * mu;  // not reached in practice
 }
 
 // Detected photons of one row and their PRF pixels; one warp per row.
@@ -315,8 +320,8 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
             const float u = rng.u();
             int c = 0;
             while (c < kComponents - 1 && u >= mix[0][c]) ++c;
-            const float ur = rng.u(), vr = rng.u();
-            const float rad = ring_radius(mix[1][c], mix[2][c], mix[3][c], ur, vr, rng);
+            const float ur = rng.u();
+            const float rad = ring_radius(mix[1][c], mix[2][c], mix[3][c], ur, rng);
             float sn, cs;
             sincospif(2.0f * rng.u(), &sn, &cs);
             for (uint32_t k = 0; k < 32; ++k) {
