@@ -616,6 +616,8 @@ def run_ours(a, rank, world, local_rank):
                          "mc_vs_mc": ev.get("mc_vs_mc"),
                          "audit": {k: st[k] for k in ("audit_events", "audit_z", "audit_radial_l1", "audit_ms")},
                          "mc_fallback_events": st["mc_events"], "surrogate_events": st["surrogate_events"],
+                         "ms": {"network_and_sampling": st["sg_ms"], "monte_carlo_outside_hull": st["mc_ms"],
+                                "audit": st["audit_ms"], "total": st["total_ms"]},
                          "model": os.path.relpath(a.surrogate_model, ROOT)}
         frontend = None
         if not a.no_frontend and world == 1:

@@ -18,7 +18,8 @@
 //      per-history counts and counters as the Monte Carlo tallies them;
 //   6. PHS and the run counter (the context's last pipeline segment);
 //   7. audit: the audited rows' depositions are transported by the Monte
-//      Carlo in label mode and compared with their predictions.
+//      Carlo in label mode, their detected photons per radial category are
+//      summed on the GPU, and the totals are compared with the predictions.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -52,6 +53,7 @@ struct RunBuffers {
     float4 *a_pos = nullptr;
     int32_t *a_n = nullptr, *a_geom = nullptr;
     double *a_pool = nullptr;  // [0, bins] sum N p q_j, then sum N p, sum N p (1 - p), sum N
+    unsigned long long *a_hist = nullptr;  // the audit's detected photons per radial category
     int64_t a_cap = 0;
     // label-mode Monte Carlo context of the audit, kept across runs
     fd2_ctx *audit = nullptr;
@@ -67,7 +69,7 @@ void sg_free_run_buffers(fd2_sg *s)
     if (!r) return;
     for (void *p : {(void *)r->d_count, (void *)r->sg_event, (void *)r->sg_n, (void *)r->audit_row, (void *)r->x0,
                     (void *)r->ha, (void *)r->hb, (void *)r->out, (void *)r->d_stat, (void *)r->a_pos,
-                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_pool})
+                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_pool, (void *)r->a_hist})
         if (p) cudaFree(p);
     fd2_destroy(r->audit);
     for (cudaEvent_t e : r->ev)
@@ -390,6 +392,26 @@ __global__ void audit_gather_kernel(const int *count, const int32_t *audit_row, 
     }
 }
 
+// Per-category totals of the audit's label-mode tally (rows [0, na) of a
+// [row][nb] array of counts): partial sums per category in shared memory,
+// then one 64-bit atomic per category and block.  Integer sums, so the
+// totals do not depend on the order.
+__global__ void radial_pool_kernel(const uint32_t *rad, int na, int nb, unsigned long long *sum)
+{
+    extern __shared__ unsigned long long s_sum[];
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) s_sum[j] = 0ull;
+    __syncthreads();
+    const long long total = (long long)na * nb;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t v = rad[i];
+        if (v) atomicAdd(&s_sum[(int)(i % nb)], (unsigned long long)v);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < nb; j += blockDim.x)
+        if (s_sum[j]) atomicAdd(&sum[j], s_sum[j]);
+}
+
 template <class T>
 cudaError_t alloc(T **p, size_t n)
 {
@@ -552,7 +574,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
                 return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "audit buffers");
             B->a_cap = na;
         }
-        if (!B->a_pool && alloc(&B->a_pool, (size_t)nb + 3))
+        if ((!B->a_pool && alloc(&B->a_pool, (size_t)nb + 3)) || (!B->a_hist && alloc(&B->a_hist, (size_t)nb)))
             return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "audit buffers");
         e = cudaMemsetAsync(B->a_pool, 0, sizeof(double) * (nb + 3), q);
         if (e == cudaSuccess) {
@@ -622,14 +644,26 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
                                       c->geoms.size() > 1 ? gg.data() : nullptr, na);
         if (st == FD2_OK) st = fd2_run(ac);
         if (st == FD2_OK) st = fd2_wait(ac);
-        std::vector<uint32_t> rad((size_t)B->audit_cap * nb);
-        if (st == FD2_OK) st = fd2_get_radial(ac, rad.data(), (int64_t)rad.size());
         if (st != FD2_OK) return sg_fail(s, st, std::string("audit Monte Carlo: ") + fd2_last_error(ac));
-        // every detected photon is in exactly one radial category
+        // every detected photon is in exactly one radial category: the
+        // categories' totals over the audited rows, pooled on the GPU
+        std::vector<unsigned long long> hsum((size_t)nb);
+        e = cudaMemsetAsync(B->a_hist, 0, sizeof(unsigned long long) * nb, ac->stream);
+        if (e == cudaSuccess) {
+            const int blocks = (int)std::max<long long>(1, std::min<long long>(4LL * s->sm_count,
+                                                                               ((long long)na * nb + 255) / 256));
+            radial_pool_kernel<<<blocks, 256, sizeof(unsigned long long) * nb, ac->stream>>>(ac->d_radial, na, nb,
+                                                                                           B->a_hist);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(hsum.data(), B->a_hist, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost,
+                                ac->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ac->stream);
+        if (e != cudaSuccess) return sg_cuda(s, e, "audit pooling");
         std::vector<double> hmc((size_t)nb, 0.0);
         double mc = 0.0;
-        for (int i = 0; i < na; ++i)
-            for (int j = 0; j < nb; ++j) hmc[(size_t)j] += rad[(size_t)i * nb + j];
+        for (int j = 0; j < nb; ++j) hmc[(size_t)j] = (double)hsum[(size_t)j];
         for (int j = 0; j < nb; ++j) mc += hmc[(size_t)j];
         const double expct = pool[(size_t)nb], var = pool[(size_t)nb + 1], ph = pool[(size_t)nb + 2];
         double ssg = 0.0, l1 = 0.0;

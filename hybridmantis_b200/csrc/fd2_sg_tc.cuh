@@ -64,8 +64,11 @@ struct TcArgs {
     long long a_split, b_split, c_split;  // element offsets of slice blockIdx.y
     unsigned *fault;  // set when a wait gives up (the tile is then not stored)
     // pipelined kernel: stage A and B with TMA (no slices) through these maps
-    // of A (K x M rows) and B (K x N rows), boxes of 8 K-elements (one 16-byte
-    // column of the canonical layout) by 128 rows (A) or N rows (B)
+    // of A (K x M rows) and B (K x N rows).  tma == 1: boxes of 8 K-elements
+    // (one 16-byte column of the no-swizzle canonical layout) by 128 rows (A)
+    // or N rows (B); tma == 2 (K a multiple of 64): boxes of 64 K-elements
+    // (128-byte rows) with the 128-byte swizzle, the K-major SWIZZLE_128B
+    // layout of the UMMA descriptors
     int tma;
     CUtensorMap tmap_a, tmap_b;
 };
@@ -84,6 +87,22 @@ __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t addr, uint32_t lbo_byt
     d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;   // stride-dimension byte offset, bits [32,46)
     d |= (uint64_t)1 << 46;                              // descriptor version for sm_100, bits [46,48)
     // base offset 0, legacy LBO mode, layout type 0 = no swizzle (bits [61,64))
+    return d;
+}
+
+// K-major SWIZZLE_128B: rows of 64 BF16 K-elements (128 bytes, their 16-byte
+// pieces XOR-permuted by row mod 8, as the TMA's 128-byte swizzle writes
+// them), 8-row groups 1024 bytes apart (SBO); the leading offset is unused
+// (1).  The groups start on 1024-byte boundaries; a K step of 16 elements
+// inside the 128-byte row advances the start address by 32 bytes.
+__device__ __forceinline__ uint64_t tc_smem_desc_sw128(uint32_t addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;            // LBO (unused), 16-byte units
+    d |= (uint64_t)(1024 >> 4) << 32;  // SBO
+    d |= (uint64_t)1 << 46;            // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;            // layout type 2 = SWIZZLE_128B
     return d;
 }
 
@@ -270,7 +289,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 
 // ---------------------------------------------------------------------------
 // Pipelined variant: the same products with the stages of consecutive tiles
-// overlapped.  Seven warps with fixed roles:
+// overlapped.  Eleven warps with fixed roles:
 //   warps 4-5 (producers): stage A in 128-row x 64-K chunks (16 KB) into a ring
 //     of four shared-memory stages with cp.async, three chunks in flight;
 //     once a chunk's copies have completed, fence.proxy.async and an arrive
@@ -281,9 +300,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 //     finished tile to its accumulator's `accf` barrier; two TMEM
 //     accumulators alternate between tiles, and a tile starts only when the
 //     epilogue has released its accumulator (`acce`);
-//   warps 0-3 (epilogue): drain their 32 TMEM lanes of a finished accumulator
-//     (tcgen05.ld, four loads of 16 columns in flight per wait), apply the
-//     epilogue (bias from shared memory), store, release the accumulator.
+//   warps 0-3 and 7-10 (epilogue): warp w drains TMEM lanes 32 (w mod 4) ..
+//     32 (w mod 4) + 31 (the lanes its position in the warpgroup may read)
+//     of a finished accumulator, warps 0-3 the even 64-column blocks and
+//     warps 7-10 the odd ones (tcgen05.ld, four loads of 16 columns in flight
+//     per wait), apply the epilogue (bias from shared memory), store, release
+//     the accumulator: two warps per scheduler, so that one's loads and
+//     stores overlap the other's arithmetic.
 //     BF16 outputs (and the ReLU mask they read) pass through a 32-row x
 //     128-byte tile per warp in shared memory, its 16-byte pieces XOR-swizzled
 //     by row so that neither the row-per-lane side nor the coalesced side has
@@ -299,8 +322,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 constexpr int kPipeStages = 4;
 constexpr int kPipeDepth = 3;  // chunks a producer lane keeps in flight (< kPipeStages)
 constexpr int kPipeProducers = 2;  // producer warps
-constexpr int kPipeThreads = 32 * (5 + kPipeProducers);  // 4 epilogue warps, the producers, 1 MMA warp
-constexpr int kPipeMmaWarp = 4 + kPipeProducers;
+constexpr int kPipeEpiWarps = 8;  // epilogue warps: two per TMEM lane quadrant
+constexpr int kPipeThreads = 32 * (kPipeEpiWarps + kPipeProducers + 1);  // epilogue, producers, 1 MMA warp
+constexpr int kPipeMmaWarp = 4 + kPipeProducers;  // warps 0-3 epilogue, 4-5 producers, 6 MMA, 7-10 epilogue
 constexpr int kPipeChunkK = 64;
 
 __host__ __device__ inline int tc_pipe_chunk(int K) { return K < kPipeChunkK ? K : kPipeChunkK; }
@@ -308,11 +332,11 @@ __host__ __device__ inline int tc_pipe_chunk(int K) { return K < kPipeChunkK ? K
 constexpr int kPipeOutBytes = 32 * 128;  // an epilogue warp's output tile: 32 rows x 64 BF16 columns
 
 // Dynamic shared memory of one CTA: B + the A ring + the epilogue warps'
-// output tiles.
+// output tiles, from the first 1024-byte boundary (the swizzled layout's).
 __host__ __device__ inline size_t tc_pipe_smem_bytes(int N, int K)
 {
-    return (size_t)N * (size_t)K * sizeof(__nv_bfloat16) +
-           (size_t)kPipeStages * kTcRows * (size_t)tc_pipe_chunk(K) * sizeof(__nv_bfloat16) + 4 * kPipeOutBytes;
+    return 1024 + (size_t)N * (size_t)K * sizeof(__nv_bfloat16) +
+           (size_t)kPipeStages * kTcRows * (size_t)tc_pipe_chunk(K) * sizeof(__nv_bfloat16) + kPipeEpiWarps * kPipeOutBytes;
 }
 
 // 16 TMEM columns of the warp's 32 lanes (no wait).
@@ -418,8 +442,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
     const __nv_bfloat16 *gA = g.A + (long long)blockIdx.y * g.a_split;
     const __nv_bfloat16 *gB = g.B + (long long)blockIdx.y * g.b_split;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char *sB = tc_smem;
-    unsigned char *sRing = tc_smem + (size_t)N * K * 2;
+    // B, then the ring, from a 1024-byte boundary: every swizzled block
+    // (B's 64-element K chunks, the ring's stages) starts on one
+    unsigned char *sB = tc_smem + ((1024u - ((uint32_t)__cvta_generic_to_shared(tc_smem) & 1023u)) & 1023u);
+    unsigned char *sRing = sB + (size_t)N * K * 2;
     const uint32_t stage_bytes = (uint32_t)(kTcRows * CK * 2);
     unsigned char *sOut = sRing + (size_t)kPipeStages * stage_bytes;
     const uint32_t acc_cols = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;
@@ -437,6 +463,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
     const uint32_t drain = (uint32_t)__cvta_generic_to_shared(&s_drain);
     const uint32_t bfull = (uint32_t)__cvta_generic_to_shared(&s_bfull);
     const bool tma = g.tma != 0;
+    const bool sw = g.tma == 2;  // SWIZZLE_128B boxes and descriptors (CK == 64)
     if (threadIdx.x == 0) {
         for (int i = 0; i < kPipeStages; ++i) {
             // the producer lanes, or (TMA) one arrive with the stage's bytes
@@ -445,7 +472,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
         }
         for (int i = 0; i < 2; ++i) {
             tc_mbar_init(accf0 + 8u * i, 1);   // one tcgen05.commit
-            tc_mbar_init(acce0 + 8u * i, 4);   // one arrive per epilogue warp
+            tc_mbar_init(acce0 + 8u * i, kPipeEpiWarps);  // one arrive per epilogue warp
         }
         tc_mbar_init(drain, 1);
         tc_mbar_init(bfull, 1);
@@ -456,7 +483,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             tc_expect_tx(bfull, (uint32_t)(N * K * 2));
             const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
-            for (int c = 0; c < K / 8; ++c) tc_tma_load(b0 + (uint32_t)(c * N * 16), &g.tmap_b, c * 8, 0, bfull);
+            if (sw)  // one box per 64-element K chunk: N rows of 128 bytes
+                for (int c = 0; c < K / 64; ++c) tc_tma_load(b0 + (uint32_t)(c * N * 128), &g.tmap_b, c * 64, 0, bfull);
+            else
+                for (int c = 0; c < K / 8; ++c) tc_tma_load(b0 + (uint32_t)(c * N * 16), &g.tmap_b, c * 8, 0, bfull);
         }
     }
     // B stays resident for all of the CTA's tiles
@@ -490,8 +520,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
                     }
                     const uint32_t dst = r0 + (uint32_t)st * stage_bytes;
                     tc_expect_tx(full0 + 8u * st, stage_bytes);
-                    for (int j = 0; j < CK / 8; ++j)
-                        tc_tma_load(dst + (uint32_t)(j * kTcRows * 16), &g.tmap_a, c * CK + j * 8, m0, full0 + 8u * st);
+                    if (sw)
+                        tc_tma_load(dst, &g.tmap_a, c * CK, m0, full0 + 8u * st);
+                    else
+                        for (int j = 0; j < CK / 8; ++j)
+                            tc_tma_load(dst + (uint32_t)(j * kTcRows * 16), &g.tmap_a, c * CK + j * 8, m0,
+                                        full0 + 8u * st);
                 }
             }
         }
@@ -560,8 +594,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t a0 = r0 + (uint32_t)st * stage_bytes;
                     for (int kk = 0; kk < CK / 16; ++kk) {
-                        const uint64_t da = tc_smem_desc(a0 + 2u * kk * lbo_a, lbo_a, 128);
-                        const uint64_t db = tc_smem_desc(b0 + (uint32_t)(c * (CK / 8) + 2 * kk) * lbo_b, lbo_b, 128);
+                        const uint64_t da = sw ? tc_smem_desc_sw128(a0 + 32u * kk)
+                                               : tc_smem_desc(a0 + 2u * kk * lbo_a, lbo_a, 128);
+                        const uint64_t db = sw ? tc_smem_desc_sw128(b0 + (uint32_t)(c * N * 128) + 32u * kk)
+                                               : tc_smem_desc(b0 + (uint32_t)(c * (CK / 8) + 2 * kk) * lbo_b, lbo_b, 128);
                         const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
@@ -589,7 +625,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warp w drains TMEM lanes (tile rows) 32w .. 32w + 31
+        // ---- epilogue: warp w drains TMEM lanes (tile rows) 32q .. 32q + 31,
+        // q = w mod 4, columns of blocks h, h + 2, ... (h = 0 for warps 0-3,
+        // 1 for warps 7-10), through output tile e of shared memory
+        const int q = warp & 3, h = warp < 4 ? 0 : 1, e = warp < 4 ? warp : warp - 3;
         int it = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
             const int a = it & 1;
@@ -604,13 +643,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int m0 = tile * kTcRows;
             const int valid = min(kTcRows, M - m0);
-            const int r = warp * 32 + lane;
+            const int r = q * 32 + lane;
             const long long row = (long long)m0 + r;
-            const uint32_t tsrc = taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)a * acc_cols;
+            const uint32_t tsrc = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)a * acc_cols;
             if ((kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) && (N & 63) == 0) {
                 // 64 columns at a time through the warp's output tile
-                unsigned char *out = sOut + (size_t)warp * kPipeOutBytes;
-                for (int c0 = 0; c0 < N; c0 += 64) {
+                unsigned char *out = sOut + (size_t)e * kPipeOutBytes;
+                for (int c0 = 64 * h; c0 < N; c0 += 128) {
                     uint32_t v[64];
                     tc_ld16(tsrc + (uint32_t)c0, v);
                     tc_ld16(tsrc + (uint32_t)c0 + 16u, v + 16);
@@ -622,8 +661,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
                         for (int i = 0; i < 8; ++i) {
                             const int rr = 4 * i + (lane >> 3), c = lane & 7;
                             uint4 mv = make_uint4(0u, 0u, 0u, 0u);
-                            if (warp * 32 + rr < valid)
-                                mv = *reinterpret_cast<const uint4 *>(g.mask + ((long long)m0 + warp * 32 + rr) * g.ldm +
+                            if (q * 32 + rr < valid)
+                                mv = *reinterpret_cast<const uint4 *>(g.mask + ((long long)m0 + q * 32 + rr) * g.ldm +
                                                                       c0 + c * 8);
                             *reinterpret_cast<uint4 *>(out + tc_out_off(rr, c)) = mv;
                         }
@@ -658,14 +697,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
                     for (int i = 0; i < 8; ++i) {
                         const int rr = 4 * i + (lane >> 3), c = lane & 7;
                         const uint4 val = *reinterpret_cast<const uint4 *>(out + tc_out_off(rr, c));
-                        if (warp * 32 + rr < valid)
+                        if (q * 32 + rr < valid)
                             *reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(g.C) +
-                                                       ((long long)m0 + warp * 32 + rr) * g.ldc + c0 + c * 8) = val;
+                                                       ((long long)m0 + q * 32 + rr) * g.ldc + c0 + c * 8) = val;
                     }
                     __syncwarp();  // the tile is read before the next columns overwrite it
                 }
             } else {
-                for (int c0 = 0; c0 < N; c0 += 16) {
+                for (int c0 = 16 * h; c0 < N; c0 += 32) {
                     uint32_t v[16];
                     tc_ld16(tsrc + (uint32_t)c0, v);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");

@@ -488,21 +488,23 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 }
 
 // A 2D map of a row-major BF16 matrix (rows x cols, row stride ld elements)
-// whose boxes are 8 columns (16 bytes) by box_rows rows: one 16-byte K column
-// of the canonical no-swizzle layout; rows past the matrix read as zeros.
-static bool encode_map(CUtensorMap *m, const __nv_bfloat16 *base, int rows, int cols, int ld, int box_rows)
+// whose boxes are box_rows rows by 8 columns (16 bytes: one K column of the
+// canonical no-swizzle layout) or, with sw128, by 64 columns (128 bytes,
+// written with the 128-byte swizzle); rows past the matrix read as zeros.
+static bool encode_map(CUtensorMap *m, const __nv_bfloat16 *base, int rows, int cols, int ld, int box_rows, bool sw128)
 {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-    if (!enc || reinterpret_cast<uintptr_t>(base) % 16 != 0 || (ld * 2) % 16 != 0 || rows < 1 || cols < 8 ||
+    const int box_cols = sw128 ? 64 : 8;
+    if (!enc || reinterpret_cast<uintptr_t>(base) % 16 != 0 || (ld * 2) % 16 != 0 || rows < 1 || cols < box_cols ||
         box_rows < 1 || box_rows > 256)
         return false;
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+               CU_TENSOR_MAP_INTERLEAVE_NONE, sw128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 cudaError_t launch_tc(fd2_sg *s, cudaStream_t st, const TcArgs &t0, unsigned grid_x, unsigned grid_y)
@@ -510,11 +512,15 @@ cudaError_t launch_tc(fd2_sg *s, cudaStream_t st, const TcArgs &t0, unsigned gri
     const dim3 grid(grid_x, grid_y);
     if (s->tc_pipe && t0.K % 16 == 0 && (t0.K <= kPipeChunkK || t0.K % kPipeChunkK == 0)) {
         // operands by TMA where the product has no batch slices and the maps
-        // can be made (16-byte aligned bases and row strides), else cp.async
+        // can be made (16-byte aligned bases and row strides), in 128-byte
+        // swizzled rows where K is a multiple of 64 (the ring's chunks are
+        // then 64 wide), else cp.async
         TcArgs t = t0;
+        const bool sw = s->tc_sw128 && t.K % 64 == 0;
         t.tma = s->tc_tma && t.a_split == 0 && t.b_split == 0 &&
-                encode_map(&t.tmap_a, t.A, t.M, t.K, t.lda, kTcRows) &&
-                encode_map(&t.tmap_b, t.B, t.N, t.K, t.ldb, t.N);
+                encode_map(&t.tmap_a, t.A, t.M, t.K, t.lda, kTcRows, sw) &&
+                encode_map(&t.tmap_b, t.B, t.N, t.K, t.ldb, t.N, sw);
+        if (t.tma && sw) t.tma = 2;
         const size_t smem = tc_pipe_smem_bytes(t.N, t.K);
         if (t.epi == kEpiBiasReluBf16) gemm_tc_pipe_kernel<kEpiBiasReluBf16><<<grid, kPipeThreads, smem, st>>>(t);
         else if (t.epi == kEpiBiasF32) gemm_tc_pipe_kernel<kEpiBiasF32><<<grid, kPipeThreads, smem, st>>>(t);
@@ -889,6 +895,7 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
         s->use_tc = !(env && std::strcmp(env, "mma") == 0);
         s->tc_pipe = !(env && std::strcmp(env, "tc1") == 0);
         s->tc_tma = !(env && std::strcmp(env, "cpasync") == 0);
+        s->tc_sw128 = !(env && std::strcmp(env, "noswizzle") == 0);
         // the tcgen05 kernels' shared memory (outside any stream capture)
         const int bytes = (int)tc_smem_bytes(kTcMaxN, kTcMaxK);
         if (cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasReluBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
