@@ -101,6 +101,7 @@ struct fd2_sg {
     bool tc_pipe = true;  // the pipelined tcgen05 kernel (FD2_SG_GEMM=tc1: the one-tile-at-a-time kernel)
     bool tc_tma = true;   // its operands by TMA where possible (FD2_SG_GEMM=cpasync: cp.async)
     bool tc_sw128 = true; // TMA boxes of 128-byte swizzled rows where K % 64 == 0 (FD2_SG_GEMM=noswizzle: 16-byte columns)
+    bool tc_tma_store = true;  // staged BF16 epilogues store by TMA (FD2_SG_GEMM=nostore: per-lane stores)
     unsigned *d_tc_fault = nullptr;
     int sm_count = 148;
 };

@@ -71,6 +71,12 @@ struct TcArgs {
     // layout of the UMMA descriptors
     int tma;
     CUtensorMap tmap_a, tmap_b;
+    // pipelined kernel, BF16 epilogues staged through shared memory: store
+    // each warp's 32-row x 64-column output block with one TMA store through
+    // this map of C (M rows x N, boxes of 64 columns x 32 rows, 128-byte
+    // swizzle: the layout of the staging tile)
+    int tma_store;
+    CUtensorMap tmap_c;
 };
 
 // Dynamic shared memory of one CTA: A tile + B.
@@ -391,6 +397,16 @@ __device__ __forceinline__ void tc_tma_load(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// TMA: one 2D box from shared memory to global memory (bulk group).
+__device__ __forceinline__ void tc_tma_store(const CUtensorMap *map, int x, int y, uint32_t src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(src)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
 // Arrive on `bar` and add `bytes` to the transfers its phase waits for.
 __device__ __forceinline__ void tc_expect_tx(uint32_t bar, uint32_t bytes)
 {
@@ -647,9 +663,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
             const long long row = (long long)m0 + r;
             const uint32_t tsrc = taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)a * acc_cols;
             if ((kEpi == kEpiBiasReluBf16 || kEpi == kEpiMaskBf16) && (N & 63) == 0) {
-                // 64 columns at a time through the warp's output tile
+                // 64 columns at a time through the warp's output tile; a warp
+                // whose 32 rows are all valid stores it with one TMA store
                 unsigned char *out = sOut + (size_t)e * kPipeOutBytes;
+                const bool bulk = g.tma_store && q * 32 + 32 <= valid;
                 for (int c0 = 64 * h; c0 < N; c0 += 128) {
+                    // the previous block's TMA store has read the tile
+                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                    __syncwarp();
                     uint32_t v[64];
                     tc_ld16(tsrc + (uint32_t)c0, v);
                     tc_ld16(tsrc + (uint32_t)c0 + 16u, v + 16);
@@ -691,6 +712,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
                             }
                         }
                         *reinterpret_cast<uint4 *>(out + tc_out_off(lane, jc)) = *reinterpret_cast<const uint4 *>(o);
+                    }
+                    if (bulk) {
+                        // the lanes' writes, visible to the async proxy, then one store
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0)
+                            tc_tma_store(&g.tmap_c, c0, m0 + q * 32, (uint32_t)__cvta_generic_to_shared(out));
+                        continue;
                     }
                     __syncwarp();
 #pragma unroll
@@ -744,6 +773,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) gemm_tc_pipe_kernel(const __g
             __syncwarp();
             if (lane == 0) tc_mbar_arrive(acce0 + 8u * a);
         }
+        // the warp's TMA stores have completed (and read their tiles)
+        if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        __syncwarp();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

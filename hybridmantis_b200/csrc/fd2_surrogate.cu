@@ -521,6 +521,10 @@ cudaError_t launch_tc(fd2_sg *s, cudaStream_t st, const TcArgs &t0, unsigned gri
                 encode_map(&t.tmap_a, t.A, t.M, t.K, t.lda, kTcRows, sw) &&
                 encode_map(&t.tmap_b, t.B, t.N, t.K, t.ldb, t.N, sw);
         if (t.tma && sw) t.tma = 2;
+        // the staged BF16 epilogues store whole 32-row blocks by TMA
+        t.tma_store = s->tc_tma_store && (t.epi == kEpiBiasReluBf16 || t.epi == kEpiMaskBf16) && t.N % 64 == 0 &&
+                      t.c_split == 0 && encode_map(&t.tmap_c, static_cast<const __nv_bfloat16 *>(t.C), t.M, t.N,
+                                                   t.ldc, 32, true);
         const size_t smem = tc_pipe_smem_bytes(t.N, t.K);
         if (t.epi == kEpiBiasReluBf16) gemm_tc_pipe_kernel<kEpiBiasReluBf16><<<grid, kPipeThreads, smem, st>>>(t);
         else if (t.epi == kEpiBiasF32) gemm_tc_pipe_kernel<kEpiBiasF32><<<grid, kPipeThreads, smem, st>>>(t);
@@ -896,6 +900,7 @@ fd2_status fd2_sg_create(const fd2_sg_config *cfg, fd2_sg **out)
         s->tc_pipe = !(env && std::strcmp(env, "tc1") == 0);
         s->tc_tma = !(env && std::strcmp(env, "cpasync") == 0);
         s->tc_sw128 = !(env && std::strcmp(env, "noswizzle") == 0);
+        s->tc_tma_store = !(env && std::strcmp(env, "nostore") == 0);
         // the tcgen05 kernels' shared memory (outside any stream capture)
         const int bytes = (int)tc_smem_bytes(kTcMaxN, kTcMaxK);
         if (cudaFuncSetAttribute(gemm_tc_kernel<kEpiBiasReluBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
