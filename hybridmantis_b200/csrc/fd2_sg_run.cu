@@ -51,7 +51,7 @@ struct RunBuffers {
     unsigned long long *d_stat = nullptr;  // [0] surrogate photons, [1] detected
     // audit: compact copies of the audited rows, pooled predictions
     float4 *a_pos = nullptr;
-    int32_t *a_n = nullptr, *a_geom = nullptr;
+    int32_t *a_n = nullptr, *a_geom = nullptr, *a_ev = nullptr;
     double *a_pool = nullptr;  // [0, bins] sum N p q_j, then sum N p, sum N p (1 - p), sum N
     unsigned long long *a_hist = nullptr;  // the audit's detected photons per radial category
     int64_t a_cap = 0;
@@ -69,7 +69,7 @@ void sg_free_run_buffers(fd2_sg *s)
     if (!r) return;
     for (void *p : {(void *)r->d_count, (void *)r->sg_event, (void *)r->sg_n, (void *)r->audit_row, (void *)r->x0,
                     (void *)r->ha, (void *)r->hb, (void *)r->out, (void *)r->d_stat, (void *)r->a_pos,
-                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_pool, (void *)r->a_hist})
+                    (void *)r->a_n, (void *)r->a_geom, (void *)r->a_ev, (void *)r->a_pool, (void *)r->a_hist})
         if (p) cudaFree(p);
     fd2_destroy(r->audit);
     for (cudaEvent_t e : r->ev)
@@ -364,31 +364,53 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
     }
 }
 
-// Compact copies of the audited rows (position, photons, geometry) and
+// Compact copies of the audited rows (position, photons, geometry, event) and
 // their pooled predictions: sum N p q_j over the radial categories j, sum N p,
-// sum N p (1 - p) and sum N (FP64 atomics; one thread per row).
+// sum N p (1 - p) and sum N (one thread per row; each warp sums its rows'
+// terms with shuffles and adds them with one FP64 atomic per term, so the
+// pool's few addresses see one atomic per 32 rows).
+__device__ __forceinline__ void warp_pool_add(double *dst, double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dst, v);
+}
+
 __global__ void audit_gather_kernel(const int *count, const int32_t *audit_row, const int32_t *sg_event,
                                     const int32_t *sg_n, const float *out, const float4 *ev_pos,
                                     const uint16_t *ev_geom, int bins, float r_max, float4 *a_pos, int32_t *a_n,
-                                    int32_t *a_geom, double *pool)
+                                    int32_t *a_geom, int32_t *a_ev, double *pool)
 {
     const int n = count[1];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int r = audit_row[i];
-        const int32_t e = sg_event[r];
-        const int32_t N = sg_n[r];
-        a_pos[i] = ev_pos[e];
-        a_n[i] = N;
-        a_geom[i] = ev_geom ? ev_geom[e] : 0;
-        const float *o = out + (int64_t)r * kOutPad;
-        const float p = 1.0f / (1.0f + expf(-o[0]));
+    const int lane = threadIdx.x & 31;
+    const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    // the warp's lanes take rows base + lane together (the shuffles need all 32)
+    for (long long base = warp0 * 32; base < n; base += nwarps * 32) {
+        const long long i = base + lane;
+        const bool live = i < n;
+        double np = 0.0, q = 0.0, nn = 0.0;
         Mix m;
-        decode_mix(o, m);
-        const double np = (double)N * p;
-        for (int j = 0; j <= bins; ++j) atomicAdd(&pool[j], np * (double)bin_prob(m, j, bins, r_max));
-        atomicAdd(&pool[bins + 1], np);
-        atomicAdd(&pool[bins + 2], np * (1.0 - (double)p));
-        atomicAdd(&pool[bins + 3], (double)N);
+        if (live) {
+            const int r = audit_row[i];
+            const int32_t e = sg_event[r];
+            const int32_t N = sg_n[r];
+            a_pos[i] = ev_pos[e];
+            a_n[i] = N;
+            a_geom[i] = ev_geom ? ev_geom[e] : 0;
+            a_ev[i] = e;
+            const float *o = out + (int64_t)r * kOutPad;
+            const float p = 1.0f / (1.0f + expf(-o[0]));
+            decode_mix(o, m);
+            np = (double)N * p;
+            q = np * (1.0 - (double)p);
+            nn = (double)N;
+        }
+        for (int j = 0; j <= bins; ++j)
+            warp_pool_add(&pool[j], live ? np * (double)bin_prob(m, j, bins, r_max) : 0.0);
+        warp_pool_add(&pool[bins + 1], np);
+        warp_pool_add(&pool[bins + 2], q);
+        warp_pool_add(&pool[bins + 3], nn);
     }
 }
 
@@ -570,7 +592,8 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
         RunBuffers *B = R;
         const int nb = s->bins + 1;
         if (na > B->a_cap) {
-            if (alloc(&B->a_pos, (size_t)na) || alloc(&B->a_n, (size_t)na) || alloc(&B->a_geom, (size_t)na))
+            if (alloc(&B->a_pos, (size_t)na) || alloc(&B->a_n, (size_t)na) || alloc(&B->a_geom, (size_t)na) ||
+                alloc(&B->a_ev, (size_t)na))
                 return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "audit buffers");
             B->a_cap = na;
         }
@@ -581,15 +604,16 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
             audit_gather_kernel<<<(unsigned)std::min((na + 127) / 128, 4096), 128, 0, q>>>(
                 R->d_count, R->audit_row, R->sg_event, R->sg_n, R->out, c->d_ev_pos,
                 c->has_geom ? c->d_ev_geom : nullptr, s->bins, (float)s->radial_max, B->a_pos, B->a_n, B->a_geom,
-                B->a_pool);
+                B->a_ev, B->a_pool);
             e = cudaGetLastError();
         }
         std::vector<float4> pos((size_t)na);
-        std::vector<int32_t> nph((size_t)na), geo((size_t)na);
+        std::vector<int32_t> nph((size_t)na), geo((size_t)na), evi((size_t)na);
         std::vector<double> pool((size_t)nb + 3);
         if (e == cudaSuccess) e = cudaMemcpyAsync(pos.data(), B->a_pos, sizeof(float4) * na, cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess) e = cudaMemcpyAsync(nph.data(), B->a_n, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess) e = cudaMemcpyAsync(geo.data(), B->a_geom, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(evi.data(), B->a_ev, sizeof(int32_t) * na, cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(pool.data(), B->a_pool, sizeof(double) * (nb + 3), cudaMemcpyDeviceToHost, q);
         if (e == cudaSuccess) e = cudaStreamSynchronize(q);
@@ -628,19 +652,27 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
             B->audit_params = c->params;
         }
         fd2_ctx *ac = B->audit;
+        // in event order: the routing kernel lists the audited rows in the
+        // order its threads reach them, and an audited event's Monte Carlo
+        // streams follow its place in the audit, so the order is fixed here
+        std::vector<uint64_t> order((size_t)na);
+        for (int i = 0; i < na; ++i) order[(size_t)i] = ((uint64_t)(uint32_t)evi[(size_t)i] << 32) | (uint32_t)i;
+        std::sort(order.begin(), order.end());
         std::vector<float> xs((size_t)na), ys((size_t)na), zs((size_t)na);
-        std::vector<int32_t> hist((size_t)na);
+        std::vector<int32_t> hist((size_t)na), nps((size_t)na);
         std::vector<uint16_t> gg((size_t)na);
-        for (int i = 0; i < na; ++i) {
-            xs[(size_t)i] = pos[(size_t)i].x;
-            ys[(size_t)i] = pos[(size_t)i].y;
-            zs[(size_t)i] = pos[(size_t)i].z;
-            hist[(size_t)i] = i + 1;
-            gg[(size_t)i] = (uint16_t)geo[(size_t)i];
+        for (int k = 0; k < na; ++k) {
+            const size_t i = (size_t)(order[(size_t)k] & 0xffffffffu);
+            xs[(size_t)k] = pos[i].x;
+            ys[(size_t)k] = pos[i].y;
+            zs[(size_t)k] = pos[i].z;
+            hist[(size_t)k] = k + 1;
+            nps[(size_t)k] = nph[i];
+            gg[(size_t)k] = (uint16_t)geo[i];
         }
         st = fd2_reset_tallies(ac);
         if (st == FD2_OK)
-            st = fd2_submit_events_um(ac, xs.data(), ys.data(), zs.data(), nullptr, hist.data(), nph.data(),
+            st = fd2_submit_events_um(ac, xs.data(), ys.data(), zs.data(), nullptr, hist.data(), nps.data(),
                                       c->geoms.size() > 1 ? gg.data() : nullptr, na);
         if (st == FD2_OK) st = fd2_run(ac);
         if (st == FD2_OK) st = fd2_wait(ac);

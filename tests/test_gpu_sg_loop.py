@@ -143,3 +143,23 @@ def test_depth_margin_routes_depositions_just_outside_the_labels(trained, tmp_pa
     n_with = with_margin["surrogate_events"] + with_margin["mc_events"]
     assert with_margin["surrogate_events"] >= 0.9 * n_with
     assert without["surrogate_events"] == 0 and without["mc_events"] == n_with
+
+
+def test_audit_is_reproducible(trained, tmp_path):
+    """The audit's Monte Carlo takes the audited events in event order, so two
+    fresh surrogates (each with its own audit context) report the same audited
+    detections on the same events, although the routing kernel lists the
+    audited rows in whatever order its threads reach them."""
+    sg, es = trained
+    path = str(tmp_path / "net.fd2sg")
+    sg.save(path)
+    res = []
+    for _ in range(2):
+        with sgm.Surrogate(hidden=256, batch=2048) as s2:
+            s2.load(path)
+            res.append(_run(es, s2, audit=0.2)["stats"])
+    a, b = res
+    assert a["audit_events"] == b["audit_events"] > 0
+    assert a["audit_mc_detected"] == b["audit_mc_detected"]
+    assert a["audit_photons"] == b["audit_photons"]
+    assert abs(a["audit_sg_expected"] - b["audit_sg_expected"]) <= 1e-9 * a["audit_sg_expected"]
