@@ -141,43 +141,63 @@ __global__ void count_kernel(int64_t n, int64_t event_base, int mode, double yie
                              int *status)
 {
     const uint32_t run_tag = *run_tag_ptr;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t k;
-        if (mode == kCountGiven) {
-            k = given_n[i];
-        } else {
-            CountRng rng{(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(event_base + i), run_tag, 0u,
-                         make_uint4(0, 0, 0, 0), 0};
-            const double mu = ev_e[i] * yield;
-            if (mode == kCountGaussian) {
-                const double u1 = rng.u(), u2 = rng.u();
-                const double zn = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-                k = (int64_t)llrint(mu + sqrt(fmax(mu, 0.0)) * zn);
+    const int lane = threadIdx.x & 31;
+    // the warp's lanes take events base + lane together, so that with one
+    // geometry the warp adds its photon total with one atomic per counter
+    // (every event adding its own count to the same two addresses
+    // serialised the kernel at millions of events)
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;  // a multiple of 32
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int64_t i = base + lane;
+        const bool live = i < n;
+        int64_t k = 0;
+        int g = 0;
+        if (live) {
+            if (mode == kCountGiven) {
+                k = given_n[i];
             } else {
-                k = poisson(rng, mu);
+                CountRng rng{(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(event_base + i), run_tag, 0u,
+                             make_uint4(0, 0, 0, 0), 0};
+                const double mu = ev_e[i] * yield;
+                if (mode == kCountGaussian) {
+                    const double u1 = rng.u(), u2 = rng.u();
+                    const double zn = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+                    k = (int64_t)llrint(mu + sqrt(fmax(mu, 0.0)) * zn);
+                } else {
+                    k = poisson(rng, mu);
+                }
+            }
+            if (k < 0) k = 0;
+            if (k > max_per_event) {
+                atomicOr(status, kStatusTooManyPhotons);
+                k = 0;
+            }
+            // an event the preparation flagged (non-finite, negative energy,
+            // history outside 1..num_hist) gets no photons: a streamed ingest
+            // queues its transport before the host sees the flag
+            const float4 p = ev_pos[i];
+            const int32_t prim = __float_as_int(p.w);
+            const double e = ev_e ? ev_e[i] : 0.0;  // no energies with given counts (fd2_transport_noalloc)
+            if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(e)) || e < 0.0 || prim < 0 || prim >= n_prim)
+                k = 0;
+            ev_n[i] = (int32_t)k;
+            ev_nchunks[i] = (uint32_t)((k + chunk - 1) / chunk);
+            g = ev_geom ? ev_geom[i] : 0;
+            if (ev_geom && k) {
+                atomicAdd(&photons_per_geom[g], (unsigned long long)k);
+                if (photons_total) atomicAdd(&photons_total[g], (unsigned long long)k);
+            }
+            if (prim_geom && prim >= 0 && prim < n_prim) prim_geom[prim] = g;
+        }
+        if (!ev_geom) {
+            unsigned long long t = (unsigned long long)k;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+            if (lane == 0 && t) {
+                atomicAdd(&photons_per_geom[0], t);
+                if (photons_total) atomicAdd(&photons_total[0], t);
             }
         }
-        if (k < 0) k = 0;
-        if (k > max_per_event) {
-            atomicOr(status, kStatusTooManyPhotons);
-            k = 0;
-        }
-        // an event the preparation flagged (non-finite, negative energy,
-        // history outside 1..num_hist) gets no photons: a streamed ingest
-        // queues its transport before the host sees the flag
-        const float4 p = ev_pos[i];
-        const int32_t prim = __float_as_int(p.w);
-        const double e = ev_e ? ev_e[i] : 0.0;  // no energies with given counts (fd2_transport_noalloc)
-        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(e)) || e < 0.0 || prim < 0 || prim >= n_prim)
-            k = 0;
-        ev_n[i] = (int32_t)k;
-        ev_nchunks[i] = (uint32_t)((k + chunk - 1) / chunk);
-        const int g = ev_geom ? ev_geom[i] : 0;
-        if (k) {
-            atomicAdd(&photons_per_geom[g], (unsigned long long)k);
-            if (photons_total) atomicAdd(&photons_total[g], (unsigned long long)k);
-        }
-        if (prim_geom && prim >= 0 && prim < n_prim) prim_geom[prim] = g;
     }
 }
 

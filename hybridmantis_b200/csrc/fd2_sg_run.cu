@@ -118,6 +118,18 @@ struct RouteArgs {
     __nv_bfloat16 *x0;
 };
 
+// ctr += 1 for each lane that reaches this point together with the calling
+// one (one atomic per group of converged lanes); returns the lane's slot.
+__device__ __forceinline__ int group_inc(int *ctr)
+{
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ctr, __popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
 __global__ void route_kernel(const RouteArgs a)
 {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -142,10 +154,10 @@ __global__ void route_kernel(const RouteArgs a)
 #pragma unroll
         for (int i = 0; i < kFeatures; ++i) in = in && f[i] >= a.hull.lo[i] && f[i] <= a.hull.hi[i];
         if (!in) {
-            atomicAdd(&a.count[2], 1);
+            group_inc(&a.count[2]);
             continue;
         }
-        const int row = atomicAdd(&a.count[0], 1);
+        const int row = group_inc(&a.count[0]);
         a.sg_event[row] = (int32_t)e;
         a.sg_n[row] = N;
         __nv_bfloat16 *x = a.x0 + (int64_t)row * kInPad;
@@ -158,7 +170,7 @@ __global__ void route_kernel(const RouteArgs a)
         a.ev_nchunks[e] = 0;
         const uint64_t ge = (uint64_t)(a.event_base + e);
         const uint4 h = philox10(make_uint4((uint32_t)ge, (uint32_t)(ge >> 32), kDomainAudit, 0), a.k0, a.k1);
-        if (unit(h.x) < a.audit_frac) a.audit_row[atomicAdd(&a.count[1], 1)] = row;
+        if (unit(h.x) < a.audit_frac) a.audit_row[group_inc(&a.count[1])] = row;
     }
 }
 
@@ -245,6 +257,17 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int rows = *a.count;
     const uint32_t run = *a.run_tag;
+    // the warp's totals over its rows (photons, detected; detected and in
+    // the PRF for the current geometry), kept by lane 0 in shared memory and
+    // added once per geometry run of rows and at the end: per-row atomics
+    // on the same four counters serialised in the L2 at millions of rows
+    __shared__ unsigned long long s_tot[kSampleThreads / 32][4];
+    __shared__ int s_tgeom[kSampleThreads / 32];
+    unsigned long long *tot = s_tot[threadIdx.x >> 5];
+    if (lane == 0) {
+        tot[0] = tot[1] = tot[2] = tot[3] = 0ull;
+        s_tgeom[threadIdx.x >> 5] = -1;
+    }
     for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
         const int64_t e = a.sg_event[r];
         const int32_t N = a.sg_n[r];
@@ -355,12 +378,28 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
             a.ev_n[e] = N;  // the run's photon count, as fd2_get_photon_counts reports it
             const int prim = __float_as_int(pos.w);
             if (total > 0 && prim >= 0 && prim < a.n_prim) atomicAdd(&a.per_primary[prim], total);
-            unsigned long long *cn = a.counters + (long long)gi * fd2::kCounterStride;
-            if (total > 0) atomicAdd(&cn[fd2::kDetect], (unsigned long long)total);
-            if (in_prf > 0) atomicAdd(&cn[fd2::kNumFates], (unsigned long long)in_prf);
-            atomicAdd(&a.stat[0], (unsigned long long)N);
-            atomicAdd(&a.stat[1], (unsigned long long)total);
+            int &tg = s_tgeom[threadIdx.x >> 5];
+            if ((int)gi != tg) {
+                if (tg >= 0) {
+                    unsigned long long *cn = a.counters + (long long)tg * fd2::kCounterStride;
+                    if (tot[2]) atomicAdd(&cn[fd2::kDetect], tot[2]);
+                    if (tot[3]) atomicAdd(&cn[fd2::kNumFates], tot[3]);
+                }
+                tg = gi;
+                tot[2] = tot[3] = 0ull;
+            }
+            tot[0] += (unsigned long long)N;
+            tot[1] += (unsigned long long)total;
+            tot[2] += (unsigned long long)total;
+            tot[3] += (unsigned long long)in_prf;
         }
+    }
+    if (lane == 0 && s_tgeom[threadIdx.x >> 5] >= 0) {
+        unsigned long long *cn = a.counters + (long long)s_tgeom[threadIdx.x >> 5] * fd2::kCounterStride;
+        if (tot[2]) atomicAdd(&cn[fd2::kDetect], tot[2]);
+        if (tot[3]) atomicAdd(&cn[fd2::kNumFates], tot[3]);
+        atomicAdd(&a.stat[0], tot[0]);
+        atomicAdd(&a.stat[1], tot[1]);
     }
 }
 
