@@ -2,9 +2,12 @@
 
 Runs the network's forward pass (fd2_sg_predict: input normalisation and the
 four GEMMs) on ``--rows`` seeded random inputs ``--runs`` times, with random
-weights of the full-size network, and prints the host time per pass.  With
-FD2_SG_GEMM=mma in the environment the GEMMs run on the mma.sync kernel
-instead of tcgen05.
+weights of the full-size network, and prints the host time per pass.
+FD2_SG_GEMM in the environment selects an earlier form of the GEMMs: ``mma``
+(mma.sync), ``tc1`` (one tcgen05 tile at a time), ``cpasync`` (pipelined,
+operands by cp.async), ``noswizzle`` (TMA boxes of 16-byte columns instead of
+128-byte swizzled rows), ``nostore`` (per-lane output stores instead of TMA
+stores).
 """
 import argparse
 import json
