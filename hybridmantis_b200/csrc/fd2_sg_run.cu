@@ -340,11 +340,18 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
             __syncwarp();
         }
         int32_t in_prf = 0;
+        // a power-of-two pixel divides exactly as a multiplication by its
+        // reciprocal (the same correctly rounded quotient)
+        const bool pow2 = (__float_as_uint(g.pixel) & 0x7fffffu) == 0u && g.pixel > 0.0f;
+        const float inv_pixel = 1.0f / g.pixel;
         for (int32_t i = lane; i < total; i += 32) {
-            // the component: the first whose cumulative weight exceeds u
+            // the component: the first whose cumulative weight exceeds u,
+            // i.e. the number of cumulative weights <= u (they do not
+            // decrease), counted without a data-dependent loop
             const float u = rng.u();
             int c = 0;
-            while (c < kComponents - 1 && u >= mix[0][c]) ++c;
+#pragma unroll
+            for (int j = 0; j < kComponents - 1; ++j) c += u >= mix[0][j] ? 1 : 0;
             const float ur = rng.u();
             const float rad = ring_radius(mix[1][c], mix[2][c], mix[3][c], ur, rng);
             float sn, cs;
@@ -364,8 +371,10 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
             }
             const float x = pos.x + rad * cs, y = pos.y + rad * sn;
             if (x <= g.ub_x && y <= g.ub_y && x >= g.lb_x && y >= g.lb_y) {
-                const int ii = (int)floorf(__fdiv_rn(x - g.lb_x, g.pixel));
-                const int jj = (int)floorf(__fdiv_rn(y - g.lb_y, g.pixel));
+                const float qx = pow2 ? __fmul_rn(x - g.lb_x, inv_pixel) : __fdiv_rn(x - g.lb_x, g.pixel);
+                const float qy = pow2 ? __fmul_rn(y - g.lb_y, inv_pixel) : __fdiv_rn(y - g.lb_y, g.pixel);
+                const int ii = (int)floorf(qx);
+                const int jj = (int)floorf(qy);
                 if (ii >= 0 && jj >= 0 && ii < g.xdim && jj < g.ydim) {
                     atomicAdd(&a.prf[g.prf_offset + (long long)ii * g.ydim + jj], 1ull);
                     ++in_prf;
