@@ -42,7 +42,8 @@ using namespace fd2::sg;
 
 struct RunBuffers {
     int64_t cap = 0;
-    int *d_count = nullptr;          // [0] surrogate rows, [1] audit rows, [2] Monte Carlo events
+    int *d_count = nullptr;          // [0] surrogate rows, [1] audit rows, [2] Monte Carlo events,
+                                     // [3] rows the sampler has handed out
     int32_t *sg_event = nullptr;     // event of each surrogate row
     int32_t *sg_n = nullptr;         // photons of each surrogate row
     int32_t *audit_row = nullptr;    // surrogate row of each audit entry
@@ -187,6 +188,7 @@ struct SampleArgs {
     int32_t n_prim;
     unsigned long long *counters;
     unsigned long long *stat;
+    int *next_row;  // rows handed out so far (zero before the launch)
     uint32_t k0, k1;
     int64_t event_base;
     const uint32_t *run_tag;
@@ -194,6 +196,7 @@ struct SampleArgs {
 };
 
 constexpr int kSampleThreads = 256;  // one warp per event
+constexpr int kRowBatch = 4;         // rows a warp takes from the counter at a time
 constexpr uint32_t kDomainLane = 0x4c414e45u;   // a lane's stream for one event
 
 // A lane's random stream for one event (its detected count and its photons'
@@ -248,13 +251,14 @@ __device__ __forceinline__ float ring_radius(float mu, float sd, float S, float 
     return 0.5f * mu;  // not reached in practice
 }
 
-// Detected photons of one row and their PRF pixels; one warp per row.
+// Detected photons of one row and their PRF pixels; one warp per row, the
+// warps taking rows from a counter in batches, so that rows of very
+// different photon counts do not leave warps idle at the end.
 __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs a)
 {
     const int lane = threadIdx.x & 31;
     __shared__ float s_mix[kSampleThreads / 32][4][kComponents];
     float(*mix)[kComponents] = s_mix[threadIdx.x >> 5];
-    const int warps = (gridDim.x * blockDim.x) >> 5;
     const int rows = *a.count;
     const uint32_t run = *a.run_tag;
     // the warp's totals over its rows (photons, detected; detected and in
@@ -268,7 +272,16 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
         tot[0] = tot[1] = tot[2] = tot[3] = 0ull;
         s_tgeom[threadIdx.x >> 5] = -1;
     }
-    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+    int r = 0, r_end = 0;  // the warp's current batch of rows
+    for (;;) {
+        if (r == r_end) {
+            int r0 = 0;
+            if (lane == 0) r0 = atomicAdd(a.next_row, kRowBatch);
+            r0 = __shfl_sync(0xffffffffu, r0, 0);
+            if (r0 >= rows) break;
+            r = r0;
+            r_end = min(r0 + kRowBatch, rows);
+        }
         const int64_t e = a.sg_event[r];
         const int32_t N = a.sg_n[r];
         const float *o = a.out + (int64_t)r * kOutPad;
@@ -402,6 +415,7 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
             tot[2] += (unsigned long long)total;
             tot[3] += (unsigned long long)in_prf;
         }
+        ++r;
     }
     if (lane == 0 && s_tgeom[threadIdx.x >> 5] >= 0) {
         unsigned long long *cn = a.counters + (long long)s_tgeom[threadIdx.x >> 5] * fd2::kCounterStride;
@@ -496,7 +510,7 @@ fd2_status ensure_run_buffers(fd2_sg *s, int64_t n)
         s->run = new RunBuffers();
         for (auto &e : s->run->ev)
             if (cudaEventCreate(&e) != cudaSuccess) return sg_fail(s, FD2_ERR_CUDA, "event create");
-        if (alloc(&s->run->d_count, 3) != cudaSuccess || alloc(&s->run->d_stat, 2) != cudaSuccess)
+        if (alloc(&s->run->d_count, 4) != cudaSuccess || alloc(&s->run->d_stat, 2) != cudaSuccess)
             return sg_fail(s, FD2_ERR_OUT_OF_MEMORY, "run buffers");
     }
     RunBuffers *r = s->run;
@@ -533,7 +547,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
     const auto t_start = std::chrono::steady_clock::now();
     const uint32_t k0 = (uint32_t)c->opt.seed ^ 0x53475255u, k1 = (uint32_t)(c->opt.seed >> 32) ^ 0x4e5f4b31u;
     cudaError_t e = cudaEventRecord(R->ev[0], q);
-    if (e == cudaSuccess) e = cudaMemsetAsync(R->d_count, 0, 3 * sizeof(int), q);
+    if (e == cudaSuccess) e = cudaMemsetAsync(R->d_count, 0, 4 * sizeof(int), q);
     if (e == cudaSuccess) e = cudaMemsetAsync(R->d_stat, 0, 2 * sizeof(unsigned long long), q);
     // 1-2: counts, routing
     if (e == cudaSuccess) e = fd2::api::count_pass(c, true);
@@ -596,6 +610,7 @@ extern "C" fd2_status fd2_sg_run(fd2_sg *s, fd2_ctx *c, double audit_fraction, f
         a.n_prim = c->n_prim;
         a.counters = c->d_counters;
         a.stat = R->d_stat;
+        a.next_row = R->d_count + 3;
         a.k0 = k0;
         a.k1 = k1;
         a.event_base = c->opt.event_base;
