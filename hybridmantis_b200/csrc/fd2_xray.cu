@@ -579,11 +579,11 @@ __device__ void source_particle(const XSource &src, XRng &r, double *p, double *
     }
 }
 
-__global__ void __launch_bounds__(128) history_kernel(XDev g, XSource src, int64_t first, int64_t n, Ede *slots,
-                                                      HistInfo *info)
+// History i of the batch (x-ray first + i): its EDEs into its slots, its
+// record into info[i].
+__device__ __forceinline__ void one_history(const XDev &g, const XSource &src, int64_t first, int64_t i, Ede *slots,
+                                            HistInfo *info)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
     XRng r(g.k0, g.k1, (uint64_t)(first + i), kStreamHistory);
     HistInfo h{};
     h.first_depth = -1.0;
@@ -617,6 +617,21 @@ __global__ void __launch_bounds__(128) history_kernel(XDev g, XSource src, int64
         }
     }
     info[i] = h;
+}
+
+// Each thread takes histories from a counter (*next, zero at launch) until
+// the batch is done: histories differ in length by orders of magnitude
+// (fluorescence, electrons), and one history per thread kept blocks
+// resident for their longest history while most of their threads idled.
+// A history's random numbers and outputs depend only on its index.
+__global__ void __launch_bounds__(128) history_kernel(XDev g, XSource src, int64_t first, int64_t n, Ede *slots,
+                                                      HistInfo *info, unsigned long long *next)
+{
+    for (;;) {
+        const int64_t i = (int64_t)atomicAdd(next, 1ull);
+        if (i >= n) return;
+        one_history(g, src, first, i, slots, info);
+    }
 }
 
 // EDE counts of a batch for the scan.
@@ -1124,7 +1139,9 @@ FD2_API fd2_status fd2_xray_create(const fd2_xray_material *m, const fd2_xray_op
         if (cudaEventCreate(&x->ev[i]) != cudaSuccess) st = FD2_ERR_CUDA;
     if (st == FD2_OK) st = upload_tables(x);
     if (st == FD2_OK && cudaMalloc(&x->d_tot, sizeof(Totals)) != cudaSuccess) st = FD2_ERR_OUT_OF_MEMORY;
-    if (st == FD2_OK && cudaMalloc(&x->d_total, sizeof(unsigned long long)) != cudaSuccess) st = FD2_ERR_OUT_OF_MEMORY;
+    // [0] a batch's EDE total, [1] the history kernel's counter
+    if (st == FD2_OK && cudaMalloc(&x->d_total, 2 * sizeof(unsigned long long)) != cudaSuccess)
+        st = FD2_ERR_OUT_OF_MEMORY;
     if (st == FD2_OK && cudaMemset(x->d_tot, 0, sizeof(Totals)) != cudaSuccess) st = FD2_ERR_CUDA;
     if (st != FD2_OK) {
         fd2_xray_destroy(x);
@@ -1179,7 +1196,8 @@ FD2_API fd2_status fd2_xray_run(fd2_xray *x, const fd2_xray_source *src, int64_t
         const unsigned grid = (unsigned)((nb + 127) / 128);
         XCUDA(x, cudaEventRecord(x->ev[0], x->stream));
         HistInfo *info = x->d_info + b0;
-        history_kernel<<<grid, 128, 0, x->stream>>>(x->dev, s, first + b0, nb, x->d_slots, info);
+        XCUDA(x, cudaMemsetAsync(x->d_total + 1, 0, sizeof(unsigned long long), x->stream));
+        history_kernel<<<grid, 128, 0, x->stream>>>(x->dev, s, first + b0, nb, x->d_slots, info, x->d_total + 1);
         XCUDA(x, cudaGetLastError());
         XCUDA(x, cudaEventRecord(x->ev[1], x->stream));
         count_kernel<<<grid, 128, 0, x->stream>>>(info, nb, x->d_counts);
