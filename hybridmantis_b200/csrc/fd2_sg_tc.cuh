@@ -7,9 +7,11 @@
 // fd2_sg_gemm.cuh) and, with the weights and the batch-major operands
 // transposed first, the backward products: input gradients dY W (mask
 // epilogue) and weight gradients dY^T X split over 256-row slices of the
-// batch (blockIdx.y = slice, FP32 partial planes).  Persistent CTAs
-// of four warps (at most one per SM) walk the 128-row tiles, the whole
-// contraction of a tile in one pass:
+// batch (blockIdx.y = slice, FP32 partial planes).  Two kernels: the
+// pipelined one (gemm_tc_pipe_kernel, below; the default) and this simple
+// one (gemm_tc_kernel), whose persistent CTAs of four warps (at most one
+// per SM) walk the 128-row tiles, the whole contraction of a tile in one
+// pass:
 //   1. the CTA stages all of B (N x K) once and, per tile, its A tile
 //      (128 x K) in shared memory (cp.async, all copies in flight together)
 //      in the canonical
@@ -31,8 +33,9 @@
 // kind::f16 (as CUTLASS's cute/arch/mma_sm100_desc.hpp spells them out).
 // Requirements: K % 16 == 0, K <= 256; N % 16 == 0, 16 <= N <= 256; row
 // strides multiples of 8 elements.  Rows past M or past *m_limit are
-// zero-filled and not stored.  No TMA and no multicast: operands are staged
-// with 16-byte cp.async copies from this GPU's memory.
+// zero-filled and not stored.  The simple kernel stages its operands with
+// 16-byte cp.async copies; the pipelined one uses TMA where it can (below).
+// No load multicasts, and every tensor map covers this GPU's memory.
 #pragma once
 
 #include <cuda.h>
@@ -297,10 +300,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 // Pipelined variant: the same products with the stages of consecutive tiles
 // overlapped.  Eleven warps with fixed roles:
 //   warps 4-5 (producers): stage A in 128-row x 64-K chunks (16 KB) into a ring
-//     of four shared-memory stages with cp.async, three chunks in flight;
-//     once a chunk's copies have completed, fence.proxy.async and an arrive
-//     on its stage's `full` barrier; it waits on the stage's `empty` barrier
-//     (the MMAs that read it have completed) before reuse;
+//     of four shared-memory stages, waiting on a stage's `empty` barrier
+//     (the MMAs that read it have completed) before reuse.  With TMA (no
+//     batch slices) one thread loads each chunk, arming the stage's `full`
+//     barrier with its bytes: one box of 64 K-elements x 128 rows in the
+//     128-byte swizzled layout where K is a multiple of 64, else one
+//     16-byte column box per 8 K-elements; B likewise, once, on its own
+//     barrier.  Otherwise both warps copy with cp.async, three chunks in
+//     flight, and mark a chunk full (after fence.proxy.async) once its
+//     copies have completed;
 //   warp 6 (one elected thread): issues the tcgen05.mma of each chunk as soon
 //     as its stage is full, commits each stage to its `empty` barrier and each
 //     finished tile to its accumulator's `accf` barrier; two TMEM
@@ -316,8 +324,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) gemm_tc_kernel(const TcArgs g)
 //     BF16 outputs (and the ReLU mask they read) pass through a 32-row x
 //     128-byte tile per warp in shared memory, its 16-byte pieces XOR-swizzled
 //     by row so that neither the row-per-lane side nor the coalesced side has
-//     bank conflicts: a warp's global store then writes four whole 128-byte
-//     row segments instead of 16 bytes of 32 rows.
+//     bank conflicts; that permutation is the TMA's 128-byte swizzle, so a
+//     warp whose 32 rows are all valid stores the tile with one TMA store,
+//     the others with coalesced 16-byte stores of whole 128-byte rows.
 // So the loads of the next chunks and the epilogue of the previous tile run
 // while the tensor core works.  B stays resident as before.  Every wait is
 // bounded (tc_wait); a role that gives up sets the fault word and leaves its
